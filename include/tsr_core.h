@@ -1,0 +1,161 @@
+/*
+ * tsr_core.h -- C ABI of the B200 (sm_100a) volumetric core of TSR.
+ *
+ * Plain pointers, sizes and opaque handles; no C++ or torch types cross this
+ * boundary.  Every entry point replaces one call site of the reference's C++
+ * scene API (paths relative to SurfaceReconstruction/SurfaceReconstruction/):
+ *
+ *   tsr_tree_build         Tree::Tree()                       Scene/Tree/Tree.cpp:26-37
+ *                          (Nodes::Nodes Nodes.cpp:186-194, Leaves::Leaves
+ *                           Leaves.cpp:22-28, DualCells::DualCells DualCells.cpp:21-31)
+ *   tsr_tree_copy_*        Tree::getNodes/getLeaves/getDualCells   Scene/Tree/Tree.h:46-57,108-121
+ *                          Nodes arrays Nodes.h:144-147, Leaves arrays Leaves.h:90-98,
+ *                          DualCells::getIndices DualCells.h:84-87
+ *   tsr_tree_copy_permutation  the in-place Samples reorder done by the tree
+ *                          (Nodes::reorderSamplesAndFillNodes Nodes.cpp:594-636)
+ *   tsr_occupancy_compute  Occupancy::Occupancy(const Tree *)   SurfaceExtraction/Occupancy.cpp:78-127
+ *   tsr_occupancy_copy     getOccupancy / getNodeStates / kernel sums, cone lengths,
+ *                          priors, cone count   Occupancy.cpp:570-597, Occupancy.h:72-86,192-210
+ *   tsr_dmc_extract        DualMarchingCells::DualMarchingCells -> extractMesh
+ *                          SurfaceExtraction/DualMarchingCells.cpp:26-169
+ *                          (the FlexibleMesh post-processing at :31-36 stays with the caller)
+ *   tsr_*_free             the owning deletes in Scene (Scene.cpp:627-670)
+ *
+ * Errors: every call returns a tsr_status; the reference throws
+ * FailureHandling::Exception instead (e.g. Nodes.cpp:238,304,405,616).
+ * tsr_last_error_message() returns the text of the last failure on the
+ * calling thread.
+ *
+ * Threading: handles are thread-compatible (one thread per handle at a time);
+ * every compute call takes the CUDA stream to run on (NULL = legacy default).
+ */
+#ifndef TSR_CORE_H
+#define TSR_CORE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define TSR_API __attribute__((visibility("default")))
+#else
+#define TSR_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    TSR_OK = 0,
+    TSR_ERR_INVALID_ARG = 1,
+    TSR_ERR_OVERFLOW_U32 = 2,   /* node / link counts beyond 32-bit indices (Nodes.cpp:399-407, Samples.h:395-402) */
+    TSR_ERR_OOM = 3,
+    TSR_ERR_CUDA = 4,
+    TSR_ERR_DEVICE_ASSERT = 5,  /* a kernel detected a broken invariant and stopped */
+    TSR_ERR_TIMEOUT = 6,        /* an iteration limit was reached */
+    TSR_ERR_STATE = 7           /* call out of order (e.g. occupancy before a tree) */
+} tsr_status;
+
+/* Parameters the reference reads from App.cfg (App.cfg:64-70); the defaults of
+ * tsr_params_default() are the shipped App.cfg values. */
+typedef struct {
+    double max_relative_sampling_distance;  /* Samples::maxRelativeSamplingDistance (h_SVO) = 2   */
+    double bandwidth_factor;                /* Occupancy::bandwidthFactor (h_O) = 2               */
+    double confidence_threshold;            /* Occupancy::confidenceThreshold = 100               */
+    double relative_radius_for_priors;      /* Occupancy::relativeRadiusForPriors = 25            */
+    double relative_sample_cone_length;     /* Occupancy::relativeSampleConeLength = 1            */
+} tsr_params;
+
+/* Structure-of-arrays view of the reference's Samples (Samples.h:300-312).
+ * All pointers are HOST memory; positions/normals are xyz-interleaved. */
+typedef struct {
+    uint32_t count;
+    uint32_t cams_per_sample;          /* K = Samples::getMaxCamerasPerSample */
+    const double *positions;           /* 3 * count */
+    const double *normals;             /* 3 * count, unit length */
+    const double *scales;              /* count, > 0 */
+    const double *confidences;         /* count */
+    const uint32_t *camera_links;      /* K * count, 0xFFFFFFFF = no camera (Cameras.cpp:29) */
+} tsr_samples_view;
+
+/* Camera centres (Cameras::getPositionWS, Cameras.h:161-166), HOST memory. */
+typedef struct {
+    uint32_t count;
+    const double *positions;           /* 3 * count */
+} tsr_cameras_view;
+
+typedef struct {
+    uint64_t nodes, leaves, dual_cells, neighbor_entries;
+    uint32_t max_depth;
+    uint32_t sampling_rounds;          /* rounds of the order-exact sampling schedule */
+    uint64_t sampling_writers;         /* sample sides that had to create nodes */
+} tsr_tree_counts;
+
+typedef struct {
+    uint64_t vertices, triangles, active_cells;
+} tsr_mesh_counts;
+
+typedef struct tsr_tree tsr_tree;
+typedef struct tsr_occupancy tsr_occupancy;
+typedef struct tsr_mesh tsr_mesh;
+
+/* Fields of tsr_occupancy_copy; scalar fields are double[leaves], node_states
+ * is uint32[nodes], cone_count is one double. */
+typedef enum {
+    TSR_FIELD_EMPTINESS_SUM = 0,   /* mKernelSums[EMPTINESS]  */
+    TSR_FIELD_SAMPLENESS_SUM = 1,  /* mKernelSums[SAMPLENESS] */
+    TSR_FIELD_EMPTINESS_LENGTH = 2,/* mConeLengths[EMPTINESS] */
+    TSR_FIELD_SAMPLENESS_LENGTH = 3,
+    TSR_FIELD_PRIOR_EMPTINESS = 4, /* mPriorsForEmptiness */
+    TSR_FIELD_OCCUPANCY = 5,       /* getOccupancy(leaf) */
+    TSR_FIELD_NODE_STATES = 6,     /* mNodeStates (uint32) */
+    TSR_FIELD_CONE_COUNT = 7       /* mConeCount */
+} tsr_field;
+
+TSR_API void tsr_params_default(tsr_params *out);
+TSR_API const char *tsr_last_error_message(void);
+TSR_API const char *tsr_version(void);
+
+TSR_API tsr_status tsr_tree_build(const tsr_samples_view *samples, const tsr_params *params,
+                          void *cuda_stream, tsr_tree **out_tree);
+TSR_API void tsr_tree_free(tsr_tree *tree);
+TSR_API tsr_status tsr_tree_get_counts(const tsr_tree *tree, tsr_tree_counts *out);
+TSR_API tsr_status tsr_tree_root_scope(const tsr_tree *tree, double min_xyz_size[4]);
+/* Node arrays after the reference's reorder; any pointer may be NULL. */
+TSR_API tsr_status tsr_tree_copy_nodes(const tsr_tree *tree, uint32_t *children, uint32_t *parents,
+                               uint32_t *sample_counts, uint32_t *sample_starts);
+/* target_indices[old sample index] = new sample index (Nodes.cpp:625-626). */
+TSR_API tsr_status tsr_tree_copy_permutation(const tsr_tree *tree, uint32_t *target_indices);
+/* scopes: 4 doubles per leaf (min x, y, z, size); node_index per leaf;
+ * node_to_leaf per node; CSR neighbour offsets (leaves + 1) and entries. */
+TSR_API tsr_status tsr_tree_copy_leaves(const tsr_tree *tree, double *scopes, uint32_t *node_index,
+                                uint32_t *node_to_leaf, uint32_t *neighbor_offsets,
+                                uint32_t *neighbors);
+TSR_API tsr_status tsr_tree_copy_dual_cells(const tsr_tree *tree, uint32_t *cells8);
+
+/* mode 0 = plain FP32 field with compensated per-leaf sums. */
+TSR_API tsr_status tsr_occupancy_compute(const tsr_tree *tree, const tsr_cameras_view *cameras,
+                                 const tsr_params *params, int mode, void *cuda_stream,
+                                 tsr_occupancy **out_occupancy);
+TSR_API void tsr_occupancy_free(tsr_occupancy *occ);
+TSR_API tsr_status tsr_occupancy_copy(const tsr_occupancy *occ, tsr_field field, void *host_dst);
+
+TSR_API tsr_status tsr_dmc_extract(const tsr_tree *tree, const tsr_occupancy *occ, void *cuda_stream,
+                           tsr_mesh **out_mesh);
+TSR_API void tsr_mesh_free(tsr_mesh *mesh);
+TSR_API tsr_status tsr_mesh_get_counts(const tsr_mesh *mesh, tsr_mesh_counts *out);
+/* cases: uint8 per dual cell; positions 3 doubles and scales 1 double per
+ * vertex; edge_keys 2 uint32 (min leaf, max leaf) per vertex; triangles 3
+ * uint32 per triangle.  Any pointer may be NULL. */
+TSR_API tsr_status tsr_mesh_copy(const tsr_mesh *mesh, uint8_t *cases, double *positions, double *scales,
+                         uint32_t *edge_keys, uint32_t *triangles);
+
+/* Wall-clock-free stage timing: CUDA-event milliseconds of the last call on
+ * this handle, per stage (see tsr_stage names in the implementation). */
+TSR_API tsr_status tsr_tree_stage_ms(const tsr_tree *tree, float *ms, int n);
+TSR_API tsr_status tsr_occupancy_stage_ms(const tsr_occupancy *occ, float *ms, int n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,141 @@
+"""GPU parity: the sm_100a path through the C ABI against the FP64 oracle.
+
+Bit-exact: root scope, node arrays, sample permutation, leaf scopes, node->leaf
+links, neighbour CSR, dual-cell list, and the DMC mesh computed from the same
+field.  Tolerance (FP32 field with compensated sums vs the FP64 oracle):
+stated per field below.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+# Tolerances of the FP32 field against the FP64 oracle.
+KSUM_RTOL = 2e-4          # kernel sums, per leaf, relative to the leaf's value
+KSUM_ATOL_REL = 1e-6      # ... plus this fraction of the largest sum
+LEN_OUTLIER_FRAC = 1e-3   # cone-length sums may differ by whole terms where a
+                          # kernel value sits on the EPSILON acceptance threshold
+PRIOR_ATOL = 1e-4
+SIGN_FLIP_FRAC = 1e-3     # leaves whose occupancy sign differs
+
+
+def _run(scene):
+    from tsr_b200 import core
+    from oracle.pyoracle import Oracle
+    o = Oracle(scene).build_tree()
+    s = core.Samples.from_scene(scene)
+    t = core.Tree(s)
+    return o, t, s
+
+
+def _check_tree(o, t):
+    c = o.counts()
+    assert t.counts["nodes"] == c["nodes"]
+    assert t.counts["leaves"] == c["leaves"]
+    assert t.counts["dual_cells"] == c["cells"]
+    assert t.counts["neighbor_entries"] == c["nbs"]
+    np.testing.assert_array_equal(t.getRootScope(), o.root())
+    on, tn = o.nodes(), t.getNodes()
+    np.testing.assert_array_equal(tn.children, on["children"])
+    np.testing.assert_array_equal(tn.parents, on["parents"])
+    np.testing.assert_array_equal(tn.samples_per_node, on["counts"])
+    np.testing.assert_array_equal(tn.sample_start_indices, on["starts"])
+    np.testing.assert_array_equal(t.getPermutation(), o.permutation())
+    ol, tl = o.leaves(), t.getLeaves()
+    np.testing.assert_array_equal(tl.scopes, ol["scopes"])
+    np.testing.assert_array_equal(tl.node_index, ol["node_idx"])
+    np.testing.assert_array_equal(tl.node_to_leaf_links, ol["node_to_leaf"])
+    np.testing.assert_array_equal(tl.neighbors_offsets, ol["nb_offsets"])
+    np.testing.assert_array_equal(tl.neighbors, ol["nbs"])
+    np.testing.assert_array_equal(t.getDualCells(), o.dual_cells())
+
+
+def test_tree_bit_exact_tiny(tiny_scene):
+    o, t, _ = _run(tiny_scene)
+    _check_tree(o, t)
+
+
+def test_tree_bit_exact_sphere(small_scene):
+    o, t, _ = _run(small_scene)
+    _check_tree(o, t)
+
+
+def test_tree_bit_exact_csg(csg_small):
+    o, t, _ = _run(csg_small)
+    _check_tree(o, t)
+
+
+def _field_errors(of, g):
+    out = {}
+    for name, key in [("emptiness_sum", "e_sum"), ("sampleness_sum", "s_sum")]:
+        a, b = g.field(name), of[key]
+        err = np.abs(a - b)
+        tol = KSUM_RTOL * np.abs(b) + KSUM_ATOL_REL * np.abs(b).max()
+        out[name] = dict(max_rel=float((err / np.maximum(np.abs(b), 1e-300)).max()),
+                         mean_rel=float((err / np.maximum(np.abs(b), 1e-300)).mean()),
+                         bad=int((err > tol).sum()))
+    return out
+
+
+def _check_field(scene, o, t):
+    from tsr_b200 import core
+    o.occupancy()
+    of = o.fields()
+    g = core.Occupancy(t, core.Cameras(scene.cams))
+    assert g.field("cone_count") == pytest.approx(of["cone_count"], rel=1e-12)
+    errs = _field_errors(of, g)
+    L = t.counts["leaves"]
+    for name, e in errs.items():
+        assert e["bad"] <= max(2, int(LEN_OUTLIER_FRAC * L)), (name, e)
+    for name, key in [("emptiness_length", "e_len"), ("sampleness_length", "s_len")]:
+        a, b = g.field(name), of[key]
+        bad = np.abs(a - b) > 1e-4 * np.abs(b) + 1e-9 * np.abs(b).max()
+        assert bad.sum() <= max(2, int(LEN_OUTLIER_FRAC * L)), (name, int(bad.sum()))
+    st = g.getNodeStates()
+    assert (st != of["states"]).sum() <= max(2, int(LEN_OUTLIER_FRAC * L))
+    pr = g.getPriorForEmptiness()
+    both = np.isfinite(pr) & np.isfinite(of["prior"])
+    assert (np.isfinite(pr) == np.isfinite(of["prior"])).mean() > 1 - LEN_OUTLIER_FRAC
+    assert np.abs(pr[both] - of["prior"][both]).max() < 5e-2
+    assert (np.abs(pr[both] - of["prior"][both]) > PRIOR_ATOL).mean() < LEN_OUTLIER_FRAC
+    occ_g, occ_o = g.getOccupancy(), of["occ"]
+    flips = ((occ_g > 0) != (occ_o > 0)).sum()
+    assert flips <= max(2, SIGN_FLIP_FRAC * L), flips
+    return g, of
+
+
+def test_field_tiny(tiny_scene):
+    o, t, _ = _run(tiny_scene)
+    _check_field(tiny_scene, o, t)
+
+
+def test_field_csg(csg_small):
+    o, t, _ = _run(csg_small)
+    _check_field(csg_small, o, t)
+
+
+def test_dmc_bit_exact_on_gpu_field(tiny_scene):
+    """The GPU mesh equals the oracle's DMC run on the GPU's own field."""
+    from tsr_b200 import core
+    o, t, _ = _run(tiny_scene)
+    g = core.Occupancy(t, core.Cameras(tiny_scene.cams))
+    m = g.extractCrust()
+    o.set_occupancy(g.getOccupancy())
+    om = o.dmc()
+    np.testing.assert_array_equal(m.cases, om["cases"])
+    np.testing.assert_array_equal(m.edge_keys, om["vkeys"])
+    np.testing.assert_array_equal(m.positions, om["vpos"])
+    np.testing.assert_array_equal(m.scales, om["vscale"])
+    np.testing.assert_array_equal(m.triangles, om["tris"])
+
+
+def test_dmc_against_fp64_field(csg_small):
+    """Case codes against the oracle's own FP64 field: differences come only
+    from sign flips of the FP32 field and are counted."""
+    from tsr_b200 import core
+    o, t, _ = _run(csg_small)
+    g, of = _check_field(csg_small, o, t)
+    m = g.extractCrust()
+    om = o.dmc()
+    diff = (m.cases != om["cases"]).mean()
+    assert diff < 5e-3, diff

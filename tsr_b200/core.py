@@ -1,0 +1,416 @@
+"""Host-side mirror of the reference's scene API over the sm_100a C ABI.
+
+The classes follow the reference's names, argument meaning and error
+behaviour (paths relative to SurfaceReconstruction/SurfaceReconstruction/):
+
+* ``Samples``            -- Scene/Samples.h:300-312 (SoA sample store)
+* ``Tree``               -- Scene/Tree/Tree.h:26-91; building it reorders the
+                            samples in place like Nodes::reorderSamplesAndFillNodes
+                            (Nodes.cpp:594-636)
+* ``Occupancy``          -- SurfaceExtraction/Occupancy.h:26-149
+* ``DualMarchingCells``  -- SurfaceExtraction/DualMarchingCells.h:31-61
+
+Every call goes through include/tsr_core.h in tsr_b200/lib/libtsrcore.so.
+There is no CPU path: if the library is missing, importing this module fails.
+Failures raise ``TsrError`` (the reference throws FailureHandling::Exception).
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+import numpy as np
+
+_LIB_PATH = Path(__file__).resolve().parent / "lib" / "libtsrcore.so"
+if not _LIB_PATH.exists():
+    raise ImportError("tsr_b200 CUDA library not built: %s (run python -m tsr_b200.build)" % _LIB_PATH)
+
+_P = ctypes.c_void_p
+_U32 = ctypes.c_uint32
+_U64 = ctypes.c_uint64
+
+
+class tsr_params(ctypes.Structure):
+    _fields_ = [("max_relative_sampling_distance", ctypes.c_double),
+                ("bandwidth_factor", ctypes.c_double),
+                ("confidence_threshold", ctypes.c_double),
+                ("relative_radius_for_priors", ctypes.c_double),
+                ("relative_sample_cone_length", ctypes.c_double)]
+
+
+class tsr_samples_view(ctypes.Structure):
+    _fields_ = [("count", _U32), ("cams_per_sample", _U32), ("positions", _P), ("normals", _P),
+                ("scales", _P), ("confidences", _P), ("camera_links", _P)]
+
+
+class tsr_cameras_view(ctypes.Structure):
+    _fields_ = [("count", _U32), ("positions", _P)]
+
+
+class tsr_tree_counts(ctypes.Structure):
+    _fields_ = [("nodes", _U64), ("leaves", _U64), ("dual_cells", _U64), ("neighbor_entries", _U64),
+                ("max_depth", _U32), ("sampling_rounds", _U32), ("sampling_writers", _U64)]
+
+
+class tsr_mesh_counts(ctypes.Structure):
+    _fields_ = [("vertices", _U64), ("triangles", _U64), ("active_cells", _U64)]
+
+
+lib = ctypes.CDLL(str(_LIB_PATH))
+_sig = {
+    "tsr_params_default": (None, [_P]),
+    "tsr_last_error_message": (ctypes.c_char_p, []),
+    "tsr_version": (ctypes.c_char_p, []),
+    "tsr_tree_build": (ctypes.c_int, [_P, _P, _P, _P]),
+    "tsr_tree_free": (None, [_P]),
+    "tsr_tree_get_counts": (ctypes.c_int, [_P, _P]),
+    "tsr_tree_root_scope": (ctypes.c_int, [_P, _P]),
+    "tsr_tree_copy_nodes": (ctypes.c_int, [_P, _P, _P, _P, _P]),
+    "tsr_tree_copy_permutation": (ctypes.c_int, [_P, _P]),
+    "tsr_tree_copy_leaves": (ctypes.c_int, [_P, _P, _P, _P, _P, _P]),
+    "tsr_tree_copy_dual_cells": (ctypes.c_int, [_P, _P]),
+    "tsr_tree_stage_ms": (ctypes.c_int, [_P, _P, ctypes.c_int]),
+    "tsr_occupancy_compute": (ctypes.c_int, [_P, _P, _P, ctypes.c_int, _P, _P]),
+    "tsr_occupancy_free": (None, [_P]),
+    "tsr_occupancy_copy": (ctypes.c_int, [_P, ctypes.c_int, _P]),
+    "tsr_occupancy_stage_ms": (ctypes.c_int, [_P, _P, ctypes.c_int]),
+    "tsr_dmc_extract": (ctypes.c_int, [_P, _P, _P, _P]),
+    "tsr_mesh_free": (None, [_P]),
+    "tsr_mesh_get_counts": (ctypes.c_int, [_P, _P]),
+    "tsr_mesh_copy": (ctypes.c_int, [_P, _P, _P, _P, _P, _P]),
+}
+for _name, (_res, _args) in _sig.items():
+    _f = getattr(lib, _name)
+    _f.restype = _res
+    _f.argtypes = _args
+
+EXPORTED = tuple(_sig)
+STATUS = {0: "TSR_OK", 1: "TSR_ERR_INVALID_ARG", 2: "TSR_ERR_OVERFLOW_U32", 3: "TSR_ERR_OOM",
+          4: "TSR_ERR_CUDA", 5: "TSR_ERR_DEVICE_ASSERT", 6: "TSR_ERR_TIMEOUT", 7: "TSR_ERR_STATE"}
+FIELDS = {"emptiness_sum": 0, "sampleness_sum": 1, "emptiness_length": 2, "sampleness_length": 3,
+          "prior_emptiness": 4, "occupancy": 5, "node_states": 6, "cone_count": 7}
+NODE_FLAG_SAMPLENESS = 1
+NODE_FLAG_EMPTINESS = 2
+INVALID_INDEX = 0xFFFFFFFF
+
+
+class TsrError(RuntimeError):
+    """Raised for a non-OK tsr_status (the reference's FailureHandling::Exception)."""
+
+    def __init__(self, status, message):
+        super().__init__("%s: %s" % (STATUS.get(status, status), message))
+        self.status = status
+
+
+def _check(rc):
+    if rc != 0:
+        raise TsrError(rc, lib.tsr_last_error_message().decode())
+
+
+def _ptr(a):
+    return a.ctypes.data_as(_P) if a is not None else None
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        return None
+    if isinstance(stream, int):
+        return _P(stream)
+    return _P(int(getattr(stream, "cuda_stream", stream)))
+
+
+def params_default():
+    p = tsr_params()
+    lib.tsr_params_default(ctypes.byref(p))
+    return p
+
+
+def make_params(h_svo=2.0, h_o=2.0, confidence_threshold=100.0, prior_radius=25.0, rel_cone_length=1.0):
+    return tsr_params(h_svo, h_o, confidence_threshold, prior_radius, rel_cone_length)
+
+
+class Samples:
+    """SoA samples (Samples.h:300-312): positions, normals, scales,
+    confidences and K camera links per sample."""
+
+    def __init__(self, positions, normals, scales, confidences, camera_links):
+        self.positions = np.ascontiguousarray(positions, np.float64).reshape(-1, 3)
+        self.normals = np.ascontiguousarray(normals, np.float64).reshape(-1, 3)
+        self.scales = np.ascontiguousarray(scales, np.float64).reshape(-1)
+        self.confidences = np.ascontiguousarray(confidences, np.float64).reshape(-1)
+        links = np.ascontiguousarray(camera_links, np.uint32)
+        self.camera_links = links.reshape(self.count, -1)
+
+    @classmethod
+    def from_scene(cls, scene):
+        return cls(scene.pos, scene.nrm, scene.scale, scene.conf, scene.links)
+
+    @property
+    def count(self):
+        return int(self.positions.shape[0])
+
+    @property
+    def max_cameras_per_sample(self):
+        return int(self.camera_links.shape[1])
+
+    def view(self):
+        return tsr_samples_view(self.count, self.max_cameras_per_sample, _ptr(self.positions), _ptr(self.normals),
+                                _ptr(self.scales), _ptr(self.confidences), _ptr(self.camera_links))
+
+    def reorder(self, target_indices):
+        """Samples::reorder (Samples.cpp:825-835): element i moves to target[i]."""
+        t = np.asarray(target_indices, np.int64)
+        for name in ("positions", "normals", "scales", "confidences", "camera_links"):
+            a = getattr(self, name)
+            b = np.empty_like(a)
+            b[t] = a
+            setattr(self, name, b)
+
+
+class Cameras:
+    """Camera centres (Cameras::getPositionWS, Cameras.h:161-166)."""
+
+    def __init__(self, positions):
+        self.positions = np.ascontiguousarray(positions, np.float64).reshape(-1, 3)
+
+    @property
+    def count(self):
+        return int(self.positions.shape[0])
+
+    def view(self):
+        return tsr_cameras_view(self.count, _ptr(self.positions))
+
+
+class Nodes:
+    """Node arrays after the reorder (Nodes.h:144-147)."""
+
+    def __init__(self, children, parents, sample_counts, sample_starts):
+        self.children = children
+        self.parents = parents
+        self.samples_per_node = sample_counts
+        self.sample_start_indices = sample_starts
+
+    def getCount(self):
+        return int(self.children.shape[0])
+
+    def isLeaf(self, node):
+        return node != INVALID_INDEX and self.children[node] == INVALID_INDEX
+
+    def getDepth(self, node):
+        d = 0
+        p = self.parents[node]
+        while p != INVALID_INDEX:
+            d += 1
+            p = self.parents[p]
+        return d
+
+
+class Leaves:
+    """Leaf scopes, node->leaf links and the neighbour CSR (Leaves.h:90-98)."""
+
+    def __init__(self, scopes, node_index, node_to_leaf, offsets, neighbors):
+        self.scopes = scopes                # (L, 4): min x, y, z, size
+        self.node_index = node_index
+        self.node_to_leaf_links = node_to_leaf
+        self.neighbors_offsets = offsets
+        self.neighbors = neighbors
+
+    def getCount(self):
+        return int(self.scopes.shape[0])
+
+    def getNeighbors(self, leaf):
+        return self.neighbors[self.neighbors_offsets[leaf]:self.neighbors_offsets[leaf + 1]]
+
+    def getCenterPositions(self):
+        return self.scopes[:, :3] + 0.5 * self.scopes[:, 3:4]
+
+
+class Tree:
+    """Tree::Tree() (Tree.cpp:26-37) on the GPU.
+
+    Like the reference, building the tree reorders ``samples`` in place so
+    that every node's samples are contiguous.
+    """
+
+    def __init__(self, samples: Samples, params=None, stream=None, reorder_samples=True):
+        self._h = _P()
+        self.params = params or params_default()
+        self._stream = stream
+        v = samples.view()
+        _check(lib.tsr_tree_build(ctypes.byref(v), ctypes.byref(self.params), _stream_ptr(stream),
+                                  ctypes.byref(self._h)))
+        c = tsr_tree_counts()
+        _check(lib.tsr_tree_get_counts(self._h, ctypes.byref(c)))
+        self.counts = {k: int(getattr(c, k)) for k, _ in tsr_tree_counts._fields_}
+        self.sample_count = samples.count
+        if reorder_samples:
+            samples.reorder(self.getPermutation())
+        self._nodes = self._leaves = self._cells = None
+
+    def __del__(self):
+        if getattr(self, "_h", None) and self._h:
+            lib.tsr_tree_free(self._h)
+            self._h = _P()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def getRootScope(self):
+        m = np.zeros(4)
+        _check(lib.tsr_tree_root_scope(self._h, _ptr(m)))
+        return m
+
+    def getRootNodeSize(self):
+        return float(self.getRootScope()[3])
+
+    def getCenter(self):
+        m = self.getRootScope()
+        return m[:3] + 0.5 * m[3]
+
+    def getPermutation(self):
+        t = np.zeros(self.sample_count, np.uint32)
+        _check(lib.tsr_tree_copy_permutation(self._h, _ptr(t)))
+        return t
+
+    def getNodes(self):
+        if self._nodes is None:
+            n = self.counts["nodes"]
+            a = [np.zeros(n, np.uint32) for _ in range(4)]
+            _check(lib.tsr_tree_copy_nodes(self._h, *[_ptr(x) for x in a]))
+            self._nodes = Nodes(*a)
+        return self._nodes
+
+    def getLeaves(self):
+        if self._leaves is None:
+            L, n, e = self.counts["leaves"], self.counts["nodes"], self.counts["neighbor_entries"]
+            scopes = np.zeros((L, 4))
+            ni = np.zeros(L, np.uint32)
+            n2l = np.zeros(n, np.uint32)
+            off = np.zeros(L + 1, np.uint32)
+            nbs = np.zeros(e, np.uint32)
+            _check(lib.tsr_tree_copy_leaves(self._h, _ptr(scopes), _ptr(ni), _ptr(n2l), _ptr(off), _ptr(nbs)))
+            self._leaves = Leaves(scopes, ni, n2l, off, nbs)
+        return self._leaves
+
+    def getDualCells(self):
+        if self._cells is None:
+            nc = self.counts["dual_cells"]
+            c = np.zeros((nc, 8), np.uint32)
+            if nc:
+                _check(lib.tsr_tree_copy_dual_cells(self._h, _ptr(c)))
+            self._cells = c
+        return self._cells
+
+    def getSampleDepth(self, scale, h_svo=None):
+        """Tree::getSampleDepth (Tree.cpp:86-91) for a sample scale."""
+        h = self.params.max_relative_sampling_distance if h_svo is None else h_svo
+        return np.ceil(np.log2(self.getRootNodeSize() / (np.asarray(scale) * h))).astype(np.uint32)
+
+    def stage_ms(self):
+        ms = np.zeros(8, np.float32)
+        _check(lib.tsr_tree_stage_ms(self._h, _ptr(ms), 8))
+        names = ["containment", "sampling", "balance", "reorder", "neighbors", "dual_cells"]
+        return {k: float(v) for k, v in zip(names, ms)}
+
+
+class Occupancy:
+    """Occupancy::Occupancy(const Tree *) (Occupancy.cpp:78-127) on the GPU."""
+
+    EMPTINESS, SAMPLENESS = 0, 1
+
+    def __init__(self, tree: Tree, cameras: Cameras, params=None, mode=0, stream=None):
+        self._h = _P()
+        self.tree = tree
+        p = params or tree.params
+        _check(lib.tsr_occupancy_compute(tree.handle, ctypes.byref(cameras.view()), ctypes.byref(p), mode,
+                                         _stream_ptr(stream), ctypes.byref(self._h)))
+        self._cache = {}
+        self.mCrust = None
+        self._stream = stream
+
+    def __del__(self):
+        if getattr(self, "_h", None) and self._h:
+            lib.tsr_occupancy_free(self._h)
+            self._h = _P()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def field(self, name):
+        if name not in self._cache:
+            if name == "cone_count":
+                v = np.zeros(1)
+            elif name == "node_states":
+                v = np.zeros(self.tree.counts["nodes"], np.uint32)
+            else:
+                v = np.zeros(self.tree.counts["leaves"])
+            _check(lib.tsr_occupancy_copy(self._h, FIELDS[name], _ptr(v)))
+            self._cache[name] = float(v[0]) if name == "cone_count" else v
+        return self._cache[name]
+
+    def getOccupancy(self, leaf=None):
+        o = self.field("occupancy")
+        return o if leaf is None else float(o[leaf])
+
+    def getNodeStates(self):
+        return self.field("node_states")
+
+    def getPriorForEmptiness(self, leaf=None):
+        p = self.field("prior_emptiness")
+        return p if leaf is None else float(p[leaf])
+
+    def getPriorForSampleness(self, leaf=None):
+        p = 1.0 - self.field("prior_emptiness")
+        return p if leaf is None else float(p[leaf])
+
+    def getEmptinessCPD(self, leaf=None):
+        v = self.field("emptiness_sum") / self.field("cone_count")
+        return v if leaf is None else float(v[leaf])
+
+    def getSamplenessCPD(self, leaf=None):
+        v = self.field("sampleness_sum") / self.field("cone_count")
+        return v if leaf is None else float(v[leaf])
+
+    def extractCrust(self, stream=None):
+        """Occupancy::extractCrust (Occupancy.cpp:523-528) without the
+        FlexibleMesh post-processing."""
+        self.mCrust = DualMarchingCells(self, stream=stream if stream is not None else self._stream)
+        return self.mCrust
+
+    def getCrust(self):
+        return self.mCrust
+
+
+class DualMarchingCells:
+    """DualMarchingCells::extractMesh (DualMarchingCells.cpp:41-169)."""
+
+    def __init__(self, occupancy: Occupancy, stream=None):
+        self._h = _P()
+        _check(lib.tsr_dmc_extract(occupancy.tree.handle, occupancy.handle, _stream_ptr(stream),
+                                   ctypes.byref(self._h)))
+        c = tsr_mesh_counts()
+        _check(lib.tsr_mesh_get_counts(self._h, ctypes.byref(c)))
+        self.counts = {k: int(getattr(c, k)) for k, _ in tsr_mesh_counts._fields_}
+        nc = occupancy.tree.counts["dual_cells"]
+        nv, nt = self.counts["vertices"], self.counts["triangles"]
+        self.cases = np.zeros(nc, np.uint8)
+        self.positions = np.zeros((nv, 3))
+        self.scales = np.zeros(nv)
+        self.edge_keys = np.zeros((nv, 2), np.uint32)
+        self.triangles = np.zeros((nt, 3), np.uint32)
+        _check(lib.tsr_mesh_copy(self._h, _ptr(self.cases), _ptr(self.positions), _ptr(self.scales),
+                                 _ptr(self.edge_keys), _ptr(self.triangles)))
+
+    def __del__(self):
+        if getattr(self, "_h", None) and self._h:
+            lib.tsr_mesh_free(self._h)
+            self._h = _P()
+
+    def getSurface(self):
+        return self.positions, self.triangles
+
+
+def version():
+    return lib.tsr_version().decode()

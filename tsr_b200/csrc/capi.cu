@@ -1,0 +1,290 @@
+// capi.cu -- extern "C" entry points of include/tsr_core.h.
+//
+// Each call validates its arguments, runs on the caller's stream, converts
+// internal failures into a tsr_status and keeps the message for
+// tsr_last_error_message() (the reference throws FailureHandling::Exception).
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "handles.h"
+
+namespace tsr {
+
+static thread_local std::string g_last_error;
+
+void fail(tsr_status st, const std::string &msg) { throw Error{st, msg}; }
+
+void check_cuda(cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return;
+    (void)cudaGetLastError();
+    tsr_status st = (e == cudaErrorMemoryAllocation) ? TSR_ERR_OOM : TSR_ERR_CUDA;
+    fail(st, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <class F>
+static tsr_status guarded(F &&f) {
+    try {
+        f();
+        return TSR_OK;
+    } catch (const Error &e) {
+        g_last_error = e.msg;
+        return e.status;
+    } catch (const std::bad_alloc &) {
+        g_last_error = "host allocation failed";
+        return TSR_ERR_OOM;
+    } catch (...) {
+        g_last_error = "unexpected failure";
+        return TSR_ERR_CUDA;
+    }
+}
+
+static void check_params(const tsr_params &p) {
+    if (!(p.max_relative_sampling_distance > 0) || !(p.bandwidth_factor > 0) ||
+        !(p.relative_radius_for_priors > 0) || !(p.relative_sample_cone_length > 0))
+        fail(TSR_ERR_INVALID_ARG, "parameters must be positive");
+}
+
+template <class T>
+static void to_host(const DBuf<T> &b, size_t n, void *dst, cudaStream_t st) {
+    if (!dst || n == 0) return;
+    TSR_CUDA(cudaMemcpyAsync(dst, b.p, n * sizeof(T), cudaMemcpyDeviceToHost, st));
+}
+
+}  // namespace tsr
+
+using namespace tsr;
+
+extern "C" {
+
+void tsr_params_default(tsr_params *out) {
+    if (!out) return;
+    out->max_relative_sampling_distance = 2.0;
+    out->bandwidth_factor = 2.0;
+    out->confidence_threshold = 100.0;
+    out->relative_radius_for_priors = 25.0;
+    out->relative_sample_cone_length = 1.0;
+}
+
+const char *tsr_last_error_message(void) { return g_last_error.c_str(); }
+
+const char *tsr_version(void) { return "tsr_b200 core 0.1 (sm_100a)"; }
+
+tsr_status tsr_tree_build(const tsr_samples_view *samples, const tsr_params *params, void *cuda_stream,
+                          tsr_tree **out_tree) {
+    if (out_tree) *out_tree = nullptr;
+    return guarded([&] {
+        if (!samples || !out_tree) fail(TSR_ERR_INVALID_ARG, "null argument");
+        if (samples->count == 0) fail(TSR_ERR_INVALID_ARG, "no samples to build a tree from (Scene.cpp:141-146)");
+        if (samples->cams_per_sample == 0) fail(TSR_ERR_INVALID_ARG, "cams_per_sample must be >= 1");
+        if (!samples->positions || !samples->normals || !samples->scales || !samples->confidences ||
+            !samples->camera_links)
+            fail(TSR_ERR_INVALID_ARG, "null sample array");
+        if ((uint64_t)samples->count * samples->cams_per_sample >= 0xFFFFFFFFull)
+            fail(TSR_ERR_OVERFLOW_U32, "link count must stay below 2^32 - 1 (Samples.h:395-402)");
+        for (uint32_t i = 0; i < samples->count; ++i)
+            if (!(samples->scales[i] > 0.0))   // Samples.cpp:280-288
+                fail(TSR_ERR_INVALID_ARG, "invalid (non-positive) sample scale at index " + std::to_string(i));
+        tsr_params p;
+        tsr_params_default(&p);
+        if (params) p = *params;
+        check_params(p);
+        tsr_tree *t = new tsr_tree();
+        t->stream = (cudaStream_t)cuda_stream;
+        t->params = p;
+        try {
+            build_tree(*t, *samples);
+        } catch (...) {
+            delete t;
+            throw;
+        }
+        *out_tree = t;
+    });
+}
+
+void tsr_tree_free(tsr_tree *tree) { delete tree; }
+
+tsr_status tsr_tree_get_counts(const tsr_tree *t, tsr_tree_counts *out) {
+    return guarded([&] {
+        if (!t || !out) fail(TSR_ERR_INVALID_ARG, "null argument");
+        out->nodes = t->n_nodes;
+        out->leaves = t->n_leaves;
+        out->dual_cells = t->n_cells;
+        out->neighbor_entries = t->n_nb;
+        out->max_depth = t->max_depth;
+        out->sampling_rounds = t->sampling_rounds;
+        out->sampling_writers = t->sampling_writers;
+    });
+}
+
+tsr_status tsr_tree_root_scope(const tsr_tree *t, double m[4]) {
+    return guarded([&] {
+        if (!t || !m) fail(TSR_ERR_INVALID_ARG, "null argument");
+        m[0] = t->root_min[0]; m[1] = t->root_min[1]; m[2] = t->root_min[2]; m[3] = t->root_size;
+    });
+}
+
+tsr_status tsr_tree_copy_nodes(const tsr_tree *t, uint32_t *children, uint32_t *parents, uint32_t *sample_counts,
+                               uint32_t *sample_starts) {
+    return guarded([&] {
+        if (!t) fail(TSR_ERR_INVALID_ARG, "null tree");
+        to_host(t->children, t->n_nodes, children, t->stream);
+        to_host(t->parents, t->n_nodes, parents, t->stream);
+        to_host(t->counts, t->n_nodes, sample_counts, t->stream);
+        to_host(t->starts, t->n_nodes, sample_starts, t->stream);
+        TSR_CUDA(cudaStreamSynchronize(t->stream));
+    });
+}
+
+tsr_status tsr_tree_copy_permutation(const tsr_tree *t, uint32_t *target) {
+    return guarded([&] {
+        if (!t || !target) fail(TSR_ERR_INVALID_ARG, "null argument");
+        to_host(t->target, t->n_samples, target, t->stream);
+        TSR_CUDA(cudaStreamSynchronize(t->stream));
+    });
+}
+
+tsr_status tsr_tree_copy_leaves(const tsr_tree *t, double *scopes, uint32_t *node_index, uint32_t *node_to_leaf,
+                                uint32_t *nb_off, uint32_t *nbs) {
+    return guarded([&] {
+        if (!t) fail(TSR_ERR_INVALID_ARG, "null tree");
+        if (scopes) {
+            std::string tmp;
+            D3 *mins = new D3[t->n_leaves ? t->n_leaves : 1];
+            uint32_t *nodes = new uint32_t[t->n_leaves ? t->n_leaves : 1];
+            uint8_t *depth = new uint8_t[t->n_nodes];
+            try {
+                to_host(t->leaf_min, t->n_leaves, mins, t->stream);
+                to_host(t->leaf_node, t->n_leaves, nodes, t->stream);
+                to_host(t->depth, t->n_nodes, depth, t->stream);
+                TSR_CUDA(cudaStreamSynchronize(t->stream));
+                for (uint32_t l = 0; l < t->n_leaves; ++l) {
+                    scopes[4 * (size_t)l + 0] = mins[l].x;
+                    scopes[4 * (size_t)l + 1] = mins[l].y;
+                    scopes[4 * (size_t)l + 2] = mins[l].z;
+                    scopes[4 * (size_t)l + 3] = size_at(t->root_size, depth[nodes[l]]);
+                }
+            } catch (...) {
+                delete[] mins; delete[] nodes; delete[] depth;
+                throw;
+            }
+            delete[] mins; delete[] nodes; delete[] depth;
+        }
+        to_host(t->leaf_node, t->n_leaves, node_index, t->stream);
+        to_host(t->node_to_leaf, t->n_nodes, node_to_leaf, t->stream);
+        to_host(t->nb_off, (size_t)t->n_leaves + 1, nb_off, t->stream);
+        to_host(t->nbs, t->n_nb, nbs, t->stream);
+        TSR_CUDA(cudaStreamSynchronize(t->stream));
+    });
+}
+
+tsr_status tsr_tree_copy_dual_cells(const tsr_tree *t, uint32_t *cells8) {
+    return guarded([&] {
+        if (!t || !cells8) fail(TSR_ERR_INVALID_ARG, "null argument");
+        to_host(t->cells, (size_t)t->n_cells * 8, cells8, t->stream);
+        TSR_CUDA(cudaStreamSynchronize(t->stream));
+    });
+}
+
+tsr_status tsr_tree_stage_ms(const tsr_tree *t, float *ms, int n) {
+    return guarded([&] {
+        if (!t || !ms) fail(TSR_ERR_INVALID_ARG, "null argument");
+        for (int i = 0; i < n && i < 8; ++i) ms[i] = t->stage_ms[i];
+    });
+}
+
+tsr_status tsr_occupancy_compute(const tsr_tree *tree, const tsr_cameras_view *cameras, const tsr_params *params,
+                                 int mode, void *cuda_stream, tsr_occupancy **out) {
+    if (out) *out = nullptr;
+    return guarded([&] {
+        if (!tree || !cameras || !out) fail(TSR_ERR_INVALID_ARG, "null argument");
+        if (cameras->count && !cameras->positions) fail(TSR_ERR_INVALID_ARG, "null camera positions");
+        if (mode != 0) fail(TSR_ERR_INVALID_ARG, "unknown occupancy mode");
+        if (tree->n_leaves == 0) fail(TSR_ERR_STATE, "tree has no leaves");
+        tsr_params p = tree->params;
+        if (params) p = *params;
+        check_params(p);
+        if (p.max_relative_sampling_distance != tree->params.max_relative_sampling_distance)
+            fail(TSR_ERR_INVALID_ARG, "h_SVO must match the tree's");
+        tsr_occupancy *o = new tsr_occupancy();
+        o->stream = (cudaStream_t)cuda_stream;
+        try {
+            compute_occupancy(*tree, *cameras, p, mode, *o);
+        } catch (...) {
+            delete o;
+            throw;
+        }
+        *out = o;
+    });
+}
+
+void tsr_occupancy_free(tsr_occupancy *o) { delete o; }
+
+tsr_status tsr_occupancy_copy(const tsr_occupancy *o, tsr_field field, void *dst) {
+    return guarded([&] {
+        if (!o || !dst) fail(TSR_ERR_INVALID_ARG, "null argument");
+        switch (field) {
+            case TSR_FIELD_EMPTINESS_SUM: to_host(o->e_sum, o->n_leaves, dst, o->stream); break;
+            case TSR_FIELD_SAMPLENESS_SUM: to_host(o->s_sum, o->n_leaves, dst, o->stream); break;
+            case TSR_FIELD_EMPTINESS_LENGTH: to_host(o->e_len, o->n_leaves, dst, o->stream); break;
+            case TSR_FIELD_SAMPLENESS_LENGTH: to_host(o->s_len, o->n_leaves, dst, o->stream); break;
+            case TSR_FIELD_PRIOR_EMPTINESS: to_host(o->prior, o->n_leaves, dst, o->stream); break;
+            case TSR_FIELD_OCCUPANCY: to_host(o->occ, o->n_leaves, dst, o->stream); break;
+            case TSR_FIELD_NODE_STATES: to_host(o->states, o->n_nodes, dst, o->stream); break;
+            case TSR_FIELD_CONE_COUNT: std::memcpy(dst, &o->cone_count, sizeof(double)); break;
+            default: fail(TSR_ERR_INVALID_ARG, "unknown field");
+        }
+        TSR_CUDA(cudaStreamSynchronize(o->stream));
+    });
+}
+
+tsr_status tsr_occupancy_stage_ms(const tsr_occupancy *o, float *ms, int n) {
+    return guarded([&] {
+        if (!o || !ms) fail(TSR_ERR_INVALID_ARG, "null argument");
+        for (int i = 0; i < n && i < 8; ++i) ms[i] = o->stage_ms[i];
+    });
+}
+
+tsr_status tsr_dmc_extract(const tsr_tree *tree, const tsr_occupancy *occ, void *cuda_stream, tsr_mesh **out) {
+    if (out) *out = nullptr;
+    return guarded([&] {
+        if (!tree || !occ || !out) fail(TSR_ERR_INVALID_ARG, "null argument");
+        if (occ->n_leaves != tree->n_leaves) fail(TSR_ERR_STATE, "occupancy does not belong to this tree");
+        tsr_mesh *m = new tsr_mesh();
+        m->stream = (cudaStream_t)cuda_stream;
+        try {
+            extract_dmc(*tree, *occ, *m);
+            TSR_CUDA(cudaStreamSynchronize(m->stream));
+        } catch (...) {
+            delete m;
+            throw;
+        }
+        *out = m;
+    });
+}
+
+void tsr_mesh_free(tsr_mesh *m) { delete m; }
+
+tsr_status tsr_mesh_get_counts(const tsr_mesh *m, tsr_mesh_counts *out) {
+    return guarded([&] {
+        if (!m || !out) fail(TSR_ERR_INVALID_ARG, "null argument");
+        out->vertices = m->n_verts;
+        out->triangles = m->n_tris;
+        out->active_cells = m->n_active;
+    });
+}
+
+tsr_status tsr_mesh_copy(const tsr_mesh *m, uint8_t *cases, double *positions, double *scales, uint32_t *edge_keys,
+                         uint32_t *triangles) {
+    return guarded([&] {
+        if (!m) fail(TSR_ERR_INVALID_ARG, "null mesh");
+        to_host(m->cases, m->n_cells, cases, m->stream);
+        to_host(m->vpos, 3 * m->n_verts, positions, m->stream);
+        to_host(m->vscale, m->n_verts, scales, m->stream);
+        to_host(m->vkeys, 2 * m->n_verts, edge_keys, m->stream);
+        to_host(m->tris, 3 * m->n_tris, triangles, m->stream);
+        TSR_CUDA(cudaStreamSynchronize(m->stream));
+    });
+}
+
+}  // extern "C"

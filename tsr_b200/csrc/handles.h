@@ -1,0 +1,61 @@
+// handles.h -- device-resident state behind the opaque C-ABI handles.
+#pragma once
+
+#include <vector>
+
+#include "common.cuh"
+
+struct tsr_tree {
+    cudaStream_t stream = nullptr;
+    tsr_params params{};
+    uint32_t n_samples = 0, k = 0;
+    double root_min[3] = {0, 0, 0};
+    double root_size = 0;
+    uint32_t n_nodes = 0, n_leaves = 0, max_depth = 0, n_cells = 0;
+    uint64_t n_nb = 0;
+    uint32_t sampling_rounds = 0;
+    uint64_t sampling_writers = 0;
+
+    // final node arrays (reference order after Nodes::reorder)
+    tsr::DBuf<uint32_t> children, parents, counts, starts;
+    tsr::DBuf<uint8_t> depth;
+    tsr::DBuf<tsr::D3> nmin;
+    tsr::DBuf<uint32_t> level_order;   // node indices sorted by depth
+    std::vector<uint32_t> level_start; // first position of each depth in level_order (+ end)
+    // samples in tree order (reordered like Samples::reorder)
+    tsr::DBuf<uint32_t> target;        // old sample index -> new
+    tsr::DBuf<tsr::D3> pos, nrm;       // FP64
+    tsr::DBuf<double> scale, conf;
+    tsr::DBuf<uint32_t> links;         // K per sample
+    // leaves
+    tsr::DBuf<tsr::D3> leaf_min;
+    tsr::DBuf<uint32_t> leaf_node, node_to_leaf, nb_off, nbs;
+    // dual cells
+    tsr::DBuf<uint32_t> cells;         // 8 per cell
+    float stage_ms[8] = {0};
+};
+
+struct tsr_occupancy {
+    cudaStream_t stream = nullptr;
+    uint32_t n_leaves = 0, n_nodes = 0;
+    tsr::DBuf<double> e_sum, s_sum, e_len, s_len, prior, occ;
+    tsr::DBuf<uint32_t> states;
+    double cone_count = 0;
+    float stage_ms[8] = {0};
+    uint64_t accepted[2] = {0, 0};
+};
+
+struct tsr_mesh {
+    cudaStream_t stream = nullptr;
+    uint64_t n_verts = 0, n_tris = 0, n_active = 0, n_cells = 0;
+    tsr::DBuf<uint8_t> cases;
+    tsr::DBuf<double> vpos, vscale;
+    tsr::DBuf<uint32_t> vkeys, tris;
+};
+
+namespace tsr {
+void build_tree(tsr_tree &t, const tsr_samples_view &sv);
+void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_params &p, int mode,
+                       tsr_occupancy &o);
+void extract_dmc(const tsr_tree &t, const tsr_occupancy &o, tsr_mesh &m);
+}  // namespace tsr

@@ -1,0 +1,416 @@
+// occupancy.cu -- sm_100a occupancy field of the TSR volumetric core.
+//
+// Reproduces Occupancy::computeOccupancy (SurfaceExtraction/Occupancy.cpp:
+// 105-127): the SAMPLENESS and EMPTINESS cone-kernel passes over every
+// camera-to-sample link (updateKernels :138-248, addKernel :279-346), the
+// bottom-up SAMPLENESS flag propagation (forwardAnyChildStateFlag :491-516),
+// the semi-local Bayesian priors (computePriors :530-568) and the per-leaf
+// occupancy value (getOccupancy :570-587).
+//
+// Precision: the per-link cone set-up, the depth cap, the cone length and the
+// cone count are FP64 (as the reference's Real = double); kernel evaluation
+// runs in FP32 in a frame centred on the sample, and every per-leaf sum is a
+// compensated FP32 pair (sum, rounding error): each atomic add returns the
+// old sum, the exact rounding error of that add (Knuth's TwoSum) goes into
+// the second word.  Priors and occupancy are evaluated in FP64 from the
+// compensated sums; the prior's sphere / box membership test is the same FP64
+// expression as the tree build's, so the set of leaves each prior sums over
+// is exact.
+#include <cub/cub.cuh>
+
+#include <vector>
+
+#include "handles.h"
+
+namespace tsr {
+namespace {
+
+constexpr unsigned BLK = 256;
+enum { EMPTINESS = 0, SAMPLENESS = 1 };
+
+struct F3 {
+    float x, y, z;
+};
+__device__ inline F3 f3(float x, float y, float z) { return F3{x, y, z}; }
+__device__ inline F3 operator-(F3 a, F3 b) { return f3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ inline F3 operator+(F3 a, F3 b) { return f3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ inline F3 operator*(F3 a, float s) { return f3(a.x * s, a.y * s, a.z * s); }
+__device__ inline float fdot(F3 a, F3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+
+// Cone in the sample-centred FP32 frame.  t is measured from the end disc:
+// te = dot(x - end, m) / denom = tComplete - 1, which keeps the arithmetic
+// near the sample (where the kernels are evaluated) well conditioned.
+struct ConeF {
+    F3 apex, end, axis, m;   // m = end-disc normal
+    float radius, full, length, inv_denom, a_over_l, t_start_e;
+    float n1, sqrt3_slack;
+};
+
+struct LinkIn {
+    const D3 *pos, *nrm;
+    const double *scale, *conf;
+    const uint32_t *links;
+    const D3 *cams;
+    uint32_t k, ncams;
+    double h_svo, h_o, rel_cone, root_size;
+};
+
+struct TreeIn {
+    const uint32_t *children;
+    const uint8_t *depth;
+    const D3 *nmin;
+    const uint32_t *node_to_leaf;
+};
+
+__device__ inline void add_comp(float2 *slot, float v) {
+    float old = atomicAdd(&slot->x, v);
+    float s = old + v;
+    float bp = s - old;
+    float err = (old - (s - bp)) + (v - bp);
+    if (err != 0.0f) atomicAdd(&slot->y, err);
+}
+
+// Conservative cone/box rejection (stands in for ObliqueCircularCone::
+// haveSeparatingAxis, ConeNodesChecker.cpp:65).  Pruning can only skip boxes
+// that contain no point of the cut cone, so the sums do not depend on it.
+__device__ inline bool cone_box_separated(const ConeF &c, F3 bmin, float size) {
+    float h = 0.5f * size;
+    F3 ctr = bmin + f3(h, h, h);
+    F3 u = ctr - c.end;
+    float te = fdot(u, c.m) * c.inv_denom;
+    float dt = h * c.n1 * fabsf(c.inv_denom);
+    float slack = 1e-4f * (dt + fabsf(te)) + 1e-6f;
+    if (te + dt < c.t_start_e - slack) return true;
+    if (te - dt >= slack) return true;
+    if (1.0f + te + dt <= 0.0f) return true;
+    F3 q = u - c.axis * te;
+    float qn = sqrtf(fdot(q, q));
+    float tmax = fminf(1.0f + te + dt, 1.0f);
+    float bound = qn - h * 1.7320508f - dt * c.full;
+    return bound > tmax * c.radius * 1.0001f + 1e-4f * (qn + h + dt * c.full);
+}
+
+// Occupancy::addKernel (Occupancy.cpp:279-346) at leaf centre x.
+__device__ inline bool eval_kernel(const ConeF &c, F3 x, bool sampleness, float conf, float *out) {
+    F3 u = x - c.end;
+    float te = fdot(u, c.m) * c.inv_denom;        // tComplete - 1
+    float tcut_m1 = te * c.a_over_l;               // tCut - 1
+    float tcut = 1.0f + tcut_m1;
+    if (tcut < 0.0f || tcut >= 1.0f) return false;
+    float tc = 1.0f + te;
+    F3 q = u - c.axis * te;                        // x - PCD centre
+    float pr = c.radius * tc;
+    float r2 = fdot(q, q);
+    float pr2 = pr * pr;
+    if (r2 >= pr2) return false;
+    float ray;
+    if (!sampleness) {
+        // Z = L, z = tCut Z: 3/(2Z) (1 - tCut^2) = 3/(2Z) (1 - tCut)(1 + tCut)
+        float Z = c.length;
+        ray = (1.5f / Z) * ((-tcut_m1) * (1.0f + tcut));
+    } else {
+        float tcen = fabsf(tcut - 0.5f) * 2.0f;
+        float Z = 0.5f * c.length;
+        if (tcen >= 1.0f) return false;
+        ray = (1.5f / Z) * (1.0f - tcen * tcen) * 0.5f;
+    }
+    float disc = (0.63661977236758134f / pr2) * (1.0f - r2 / pr2);
+    float kv = ray * disc;
+    if (!(kv >= (float)EPS)) return false;
+    float scaled = conf * kv;
+    if (!(scaled >= (float)EPS)) return false;
+    *out = scaled;
+    return true;
+}
+
+__device__ inline F3 rel(const D3 &a, const D3 &origin) {
+    return f3((float)(a.x - origin.x), (float)(a.y - origin.y), (float)(a.z - origin.z));
+}
+
+// One thread per camera-to-sample link (Occupancy.cpp:170-236).
+template <int TYPE>
+__global__ void __launch_bounds__(128) k_cone_pass(uint64_t nlinks, LinkIn in, TreeIn tr, uint32_t *states,
+                                                   float2 *ksum, float2 *clen, double *cone_count,
+                                                   unsigned long long *accepted, int *err) {
+    uint64_t l = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    double count = 0.0;
+    unsigned long long acc = 0;
+    if (l < nlinks) do {
+        uint32_t s = (uint32_t)(l / in.k);
+        uint32_t cam = in.links[l];
+        if (cam == INVALID || cam >= in.ncams) break;
+        D3 p = in.pos[s];
+        D3 n = in.nrm[s];
+        D3 cw = in.cams[cam];
+        double kernel_r = in.h_o * in.scale[s];
+        // FP64 cone set-up (Occupancy.cpp:180-201)
+        D3 apex_d{cw.x - p.x, cw.y - p.y, cw.z - p.z};   // apex relative to the sample
+        D3 end_d{0.0, 0.0, 0.0};
+        double cone_len = REAL_MAX;
+        if (TYPE == SAMPLENESS) {
+            D3 cs{-apex_d.x, -apex_d.y, -apex_d.z};
+            double total = sqrt(cs.x * cs.x + cs.y * cs.y + cs.z * cs.z);
+            cone_len = kernel_r * in.rel_cone;
+            double h = cone_len * 0.5;
+            end_d = D3{cs.x / total * h, cs.y / total * h, cs.z / total * h};
+        }
+        D3 m{-n.x, -n.y, -n.z};
+        D3 axis{end_d.x - apex_d.x, end_d.y - apex_d.y, end_d.z - apex_d.z};
+        double full = sqrt(axis.x * axis.x + axis.y * axis.y + axis.z * axis.z);
+        double length = cone_len < full ? cone_len : full;
+        double denom = axis.x * m.x + axis.y * m.y + axis.z * m.z;
+        if (!(full > EPS) || !(kernel_r > 0.0) || fabs(denom) <= EPS * full) break;   // isDegenerated
+        double conf = in.conf[s];
+        if (TYPE == EMPTINESS) count = conf;
+        float wlen = (float)(conf * length);
+        double depth_d = ceil(log2(in.root_size / (in.scale[s] * in.h_svo)));   // Tree.cpp:86-91
+        uint32_t max_depth = (uint32_t)depth_d + MAX_DEPTH_DIFFERENCE;
+        ConeF c;
+        c.apex = f3((float)apex_d.x, (float)apex_d.y, (float)apex_d.z);
+        c.end = f3((float)end_d.x, (float)end_d.y, (float)end_d.z);
+        c.axis = f3((float)axis.x, (float)axis.y, (float)axis.z);
+        c.m = f3((float)m.x, (float)m.y, (float)m.z);
+        c.radius = (float)kernel_r;
+        c.full = (float)full;
+        c.length = (float)length;
+        c.inv_denom = (float)(1.0 / denom);
+        c.a_over_l = (float)(full / length);
+        c.t_start_e = (float)(-length / full);   // tComplete - 1 at the cut start
+        c.n1 = fabsf(c.m.x) + fabsf(c.m.y) + fabsf(c.m.z);
+        const float fconf = (float)conf;
+        const uint32_t req = (TYPE == EMPTINESS) ? FLAG_SAMPLENESS : 0u;
+        const uint32_t leaf_flag = (TYPE == EMPTINESS) ? FLAG_EMPTINESS : FLAG_SAMPLENESS;
+        const float root_size_f = (float)in.root_size;
+
+        // LeavesIterator with ConeNodesChecker (NodesIterator.cpp:38-86)
+        auto ignored = [&](uint32_t node, F3 bmin, float size) -> bool {
+            if (req && (states[node] & req) != req) return true;
+            return cone_box_separated(c, bmin, size);
+        };
+        auto visit_leaf = [&](uint32_t node, F3 bmin, float size) {
+            float h = 0.5f * size;
+            float val;
+            if (!eval_kernel(c, bmin + f3(h, h, h), TYPE == SAMPLENESS, fconf, &val)) return;
+            uint32_t leaf = tr.node_to_leaf[node];
+            add_comp(&ksum[leaf], val);
+            add_comp(&clen[leaf], wlen);
+            if ((states[node] & leaf_flag) == 0) atomicOr(&states[node], leaf_flag);
+            ++acc;
+        };
+        F3 rmin = rel(tr.nmin[0], p);
+        if (ignored(0, rmin, root_size_f)) break;
+        if (tr.children[0] == INVALID) { visit_leaf(0, rmin, root_size_f); break; }
+        uint32_t st_node[MAX_TREE_DEPTH];
+        uint8_t st_next[MAX_TREE_DEPTH];
+        int sp = 1;
+        st_node[0] = 0;
+        st_next[0] = 0;
+        while (sp > 0) {
+            int t = sp - 1;
+            if (st_next[t] == 8) { --sp; continue; }
+            uint32_t ci = st_next[t]++;
+            uint32_t idx = tr.children[st_node[t]] + ci;
+            uint32_t d = (uint32_t)t + 1;   // depth of the child
+            float size = ldexpf(root_size_f, -(int)d);
+            F3 bmin = rel(tr.nmin[idx], p);
+            if (ignored(idx, bmin, size)) continue;
+            if (tr.children[idx] == INVALID) { visit_leaf(idx, bmin, size); continue; }
+            if (d + 1 > max_depth) continue;   // goDown stops at the depth cap
+            if (sp >= MAX_TREE_DEPTH) { atomicExch(err, 1); break; }
+            st_node[sp] = idx;
+            st_next[sp] = 0;
+            ++sp;
+        }
+    } while (0);
+    // block-level reduction of the cone count and the accepted counter
+    typedef cub::BlockReduce<double, 128> BR;
+    typedef cub::BlockReduce<unsigned long long, 128> BRU;
+    __shared__ typename BR::TempStorage tmp;
+    __shared__ typename BRU::TempStorage tmpu;
+    double bc = BR(tmp).Sum(count);
+    unsigned long long ba = BRU(tmpu).Sum(acc);
+    if (threadIdx.x == 0) {
+        if (TYPE == EMPTINESS && bc != 0.0) atomicAdd(cone_count, bc);
+        if (ba) atomicAdd(accepted, ba);
+    }
+}
+
+// forwardAnyChildStateFlag, one level bottom-up.
+__global__ void k_forward_flag(uint32_t lo, uint32_t hi, const uint32_t *order, const uint32_t *children,
+                               uint32_t *states, uint32_t flag) {
+    uint32_t i = lo + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= hi) return;
+    uint32_t n = order[i];
+    uint32_t c0 = children[n];
+    if (c0 == INVALID) return;
+    uint32_t s = states[n] & ~flag;
+    for (uint32_t c = 0; c < 8; ++c)
+        if (states[c0 + c] & flag) s |= flag;
+    states[n] = s;
+}
+
+__device__ inline double comp_value(float2 v) { return (double)v.x + (double)v.y; }
+
+// Occupancy::computePriors (Occupancy.cpp:530-568) with a
+// SphereNodeStatesChecker (SphereNodeStatesChecker.cpp:28-36).
+__global__ void __launch_bounds__(128) k_priors(uint32_t nl, const uint32_t *leaf_node, const D3 *leaf_min,
+                                                TreeIn tr, const uint32_t *states, const float2 *elen,
+                                                const float2 *slen, double root_size, double rel_radius,
+                                                double *prior, int *err) {
+    uint32_t l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= nl) return;
+    uint32_t node = leaf_node[l];
+    uint32_t ld = tr.depth[node];
+    double size = size_at(root_size, ld);
+    D3 mn = leaf_min[l];
+    double half = dmul(0.5, size);
+    D3 center{dadd(mn.x, half), dadd(mn.y, half), dadd(mn.z, half)};
+    double radius = dmul(size, rel_radius);
+    uint32_t max_depth = ld + MAX_DEPTH_DIFFERENCE;
+    double eL = 0.0, sL = 0.0;
+    auto ignored = [&](uint32_t n, double sz, uint32_t depth) -> bool {
+        if ((states[n] & FLAG_SAMPLENESS) == 0) return true;
+        if (depth > max_depth) return true;
+        D3 bmn = tr.nmin[n];
+        D3 bmx{dadd(bmn.x, sz), dadd(bmn.y, sz), dadd(bmn.z, sz)};
+        return !aabb_sphere(bmn, bmx, center, radius);
+    };
+    auto visit = [&](uint32_t n) {
+        uint32_t leaf = tr.node_to_leaf[n];
+        eL += comp_value(elen[leaf]);
+        sL += comp_value(slen[leaf]);
+    };
+    if (!ignored(0, root_size, 0)) {
+        if (tr.children[0] == INVALID) {
+            visit(0);
+        } else {
+            uint32_t st_node[MAX_TREE_DEPTH];
+            uint8_t st_next[MAX_TREE_DEPTH];
+            int sp = 1;
+            st_node[0] = 0;
+            st_next[0] = 0;
+            while (sp > 0) {
+                int t = sp - 1;
+                if (st_next[t] == 8) { --sp; continue; }
+                uint32_t ci = st_next[t]++;
+                uint32_t idx = tr.children[st_node[t]] + ci;
+                uint32_t d = (uint32_t)t + 1;
+                double sz = size_at(root_size, d);
+                if (ignored(idx, sz, d)) continue;
+                if (tr.children[idx] == INVALID) { visit(idx); continue; }
+                if (d + 1 > max_depth) continue;
+                if (sp >= MAX_TREE_DEPTH) { atomicExch(err, 2); break; }
+                st_node[sp] = idx;
+                st_next[sp] = 0;
+                ++sp;
+            }
+        }
+    }
+    prior[l] = eL / (eL + sL);
+}
+
+// Occupancy::getOccupancy (Occupancy.cpp:570-587), FP64.
+__global__ void k_finalize(uint32_t nl, const float2 *esum, const float2 *ssum, const float2 *elen,
+                           const float2 *slen, const double *prior, double cone_count, double threshold,
+                           double *o_esum, double *o_ssum, double *o_elen, double *o_slen, double *occ) {
+    uint32_t l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= nl) return;
+    double e = comp_value(esum[l]), s = comp_value(ssum[l]);
+    o_esum[l] = e;
+    o_ssum[l] = s;
+    o_elen[l] = comp_value(elen[l]);
+    o_slen[l] = comp_value(slen[l]);
+    double v;
+    if ((e + s) < threshold) {
+        v = -EPS;
+    } else {
+        double pr = prior[l];
+        double pe = pr * (e / cone_count);
+        double ps = (1.0 - pr) * (s / cone_count);
+        v = (pe >= ps) ? -EPS : ps - pe;
+    }
+    occ[l] = v;
+}
+
+struct Timer {
+    cudaEvent_t a{}, b{};
+    cudaStream_t st;
+    explicit Timer(cudaStream_t s) : st(s) {
+        TSR_CUDA(cudaEventCreate(&a));
+        TSR_CUDA(cudaEventCreate(&b));
+        TSR_CUDA(cudaEventRecord(a, st));
+    }
+    float lap() {
+        TSR_CUDA(cudaEventRecord(b, st));
+        TSR_CUDA(cudaEventSynchronize(b));
+        float ms = 0;
+        TSR_CUDA(cudaEventElapsedTime(&ms, a, b));
+        std::swap(a, b);
+        return ms;
+    }
+    ~Timer() { cudaEventDestroy(a); cudaEventDestroy(b); }
+};
+
+}  // namespace
+
+void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_params &p, int mode,
+                       tsr_occupancy &o) {
+    (void)mode;
+    cudaStream_t st = o.stream;
+    const uint32_t nl = t.n_leaves, nn = t.n_nodes;
+    o.n_leaves = nl;
+    o.n_nodes = nn;
+    Timer timer(st);
+    DBuf<D3> cams(cv.count, st);
+    if (cv.count) TSR_CUDA(cudaMemcpyAsync(cams.p, cv.positions, (size_t)cv.count * 24, cudaMemcpyHostToDevice, st));
+    DBuf<float2> acc(4ull * nl, st);   // esum, ssum, elen, slen
+    acc.zero();
+    float2 *esum = acc.p, *ssum = acc.p + nl, *elen = acc.p + 2ull * nl, *slen = acc.p + 3ull * nl;
+    o.states.alloc(nn, st);
+    o.states.zero();
+    DBuf<double> cone_count(1, st);
+    cone_count.zero();
+    DBuf<unsigned long long> accepted(2, st);
+    accepted.zero();
+    DBuf<int> err(1, st);
+    err.zero();
+
+    LinkIn in{t.pos.p, t.nrm.p, t.scale.p, t.conf.p, t.links.p, cams.p, t.k, cv.count,
+              p.max_relative_sampling_distance, p.bandwidth_factor, p.relative_sample_cone_length, t.root_size};
+    TreeIn tr{t.children.p, t.depth.p, t.nmin.p, t.node_to_leaf.p};
+    uint64_t nlinks = (uint64_t)t.n_samples * t.k;
+    unsigned grid = (unsigned)((nlinks + 127) / 128);
+    if (grid == 0) grid = 1;
+    k_cone_pass<SAMPLENESS><<<grid, 128, 0, st>>>(nlinks, in, tr, o.states.p, ssum, slen, cone_count.p, accepted.p + 1,
+                                                  err.p);
+    o.stage_ms[0] = timer.lap();
+    // forwardAnyChildStateFlag(0, SAMPLENESS) before the EMPTINESS pass (Occupancy.cpp:141-142)
+    for (int d = (int)t.level_start.size() - 2; d >= 0; --d) {
+        uint32_t lo = t.level_start[d], hi = t.level_start[d + 1];
+        k_forward_flag<<<grid_for(hi - lo, BLK), BLK, 0, st>>>(lo, hi, t.level_order.p, t.children.p, o.states.p,
+                                                              FLAG_SAMPLENESS);
+    }
+    o.stage_ms[1] = timer.lap();
+    k_cone_pass<EMPTINESS><<<grid, 128, 0, st>>>(nlinks, in, tr, o.states.p, esum, elen, cone_count.p, accepted.p,
+                                                 err.p);
+    o.stage_ms[2] = timer.lap();
+    o.prior.alloc(nl, st);
+    k_priors<<<grid_for(nl, 128), 128, 0, st>>>(nl, t.leaf_node.p, t.leaf_min.p, tr, o.states.p, elen, slen,
+                                               t.root_size, p.relative_radius_for_priors, o.prior.p, err.p);
+    o.stage_ms[3] = timer.lap();
+    o.cone_count = read_scalar(cone_count.p, st);
+    o.e_sum.alloc(nl, st); o.s_sum.alloc(nl, st); o.e_len.alloc(nl, st); o.s_len.alloc(nl, st); o.occ.alloc(nl, st);
+    k_finalize<<<grid_for(nl, BLK), BLK, 0, st>>>(nl, esum, ssum, elen, slen, o.prior.p, o.cone_count,
+                                                 p.confidence_threshold, o.e_sum.p, o.s_sum.p, o.e_len.p, o.s_len.p,
+                                                 o.occ.p);
+    o.stage_ms[4] = timer.lap();
+    unsigned long long a[2];
+    TSR_CUDA(cudaMemcpyAsync(a, accepted.p, 16, cudaMemcpyDeviceToHost, st));
+    int e = read_scalar(err.p, st);
+    o.accepted[0] = a[0];
+    o.accepted[1] = a[1];
+    if (e) fail(TSR_ERR_DEVICE_ASSERT, "occupancy traversal exceeded its stack bound");
+    TSR_CUDA(cudaGetLastError());
+}
+
+}  // namespace tsr
