@@ -1,0 +1,332 @@
+#!/usr/bin/env python
+"""Throughput of the TSR volumetric core (octree + occupancy field + dual
+marching cells) on B200, in samples/s.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload csg4m|sphere|heldout16m]
+
+A step is one reconstruction of the workload's samples: tree build, both
+cone-kernel passes, priors, occupancy values and DMC.
+
+* ``value``  -- samples resident in HBM when the timed region starts
+  (tsr_tree_build_device), CUDA events on the launching stream.
+* ``e2e``    -- the same step through the public API (tsr_b200.core.Tree /
+  Occupancy / extractCrust) from pinned host buffers: H2D of the samples and
+  the cameras, and the mesh (case codes, vertices, triangles) copied back,
+  every step.
+* ``--impl reference`` -- the FP64 CPU oracle (a restatement of the reference's
+  C++ path, which cannot be built here) on the host cores, same metric.
+
+Multi-GPU: replicas only (each rank reconstructs its own seeded scene; there
+is no data-path collective); value = all ranks' samples / max rank time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "samples/s (octree+occupancy+DMC) MLP-pruned vs plain FP32 on B200, fixed mesh error"
+UNIT = "samples/s"
+L2_BYTES = 126 * 1024 * 1024
+CPU_SAMPLE_N = 60_000
+
+
+def make_scene(workload, seed):
+    from tsr_b200 import scenes
+    if workload == "csg4m":
+        return scenes.csg_scene(seed=seed, n_target=4_000_000), \
+            "csg: 2 mm plate + cylinder r=0.3 + torus R=0.5/r=0.1, 120 cameras at 1.5-12, 4M samples"
+    if workload == "sphere":
+        return scenes.sphere_scene(seed=seed, stride=3), "unit sphere, 24 cameras, ~250k samples"
+    if workload == "heldout16m":
+        return scenes.random_csg_scene(seed=999 + seed, n_target=16_000_000, width=1600, height=1200, f=1200.0), \
+            "held-out random CSG scene, 16M samples"
+    raise SystemExit("unknown workload " + workload)
+
+
+def cpu_scene(workload):
+    from tsr_b200 import scenes
+    if workload == "sphere":
+        return scenes.sphere_scene(stride=9)
+    return scenes.csg_scene(seed=0, n_target=CPU_SAMPLE_N)
+
+
+def run_oracle_once(scene, threads):
+    from oracle.pyoracle import Oracle
+    t0 = time.perf_counter()
+    o = Oracle(scene)
+    o.build_tree()
+    o.occupancy(nthreads=threads)
+    o.dmc()
+    return time.perf_counter() - t0
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.p = None
+        self.path = ROOT / "gpurun_out" / ("clocks_%d.csv" % index)
+
+    def start(self):
+        try:
+            self.path.parent.mkdir(exist_ok=True)
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if not self.p:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(5)
+        except Exception:
+            self.p.kill()
+        self.f.close()
+        rows = []
+        for line in self.path.read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    scene = cpu_scene(args.workload)
+    for _ in range(args.warmup):
+        run_oracle_once(scene, threads)
+    times = [run_oracle_once(scene, threads) for _ in range(args.steps)]
+    t = sum(times)
+    value = scene.n * args.steps / t
+    sample = "oracle full pipeline (tree, occupancy, priors, DMC) on the %s workload's geometry and cameras " \
+             "at %d samples" % (args.workload, scene.n)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": args.workload, "samples": scene.n},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def our_arm(args):
+    import ctypes
+
+    import numpy as np
+    import torch
+    from tsr_b200 import core
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    scene, desc = make_scene(args.workload, seed=rank)
+    n = scene.n
+    stream = torch.cuda.current_stream()
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+    params = core.params_default()
+    cams = core.Cameras(scene.cams)
+
+    # ---- device-resident inputs for the `value` leg
+    dev = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in
+           dict(pos=scene.pos, nrm=scene.nrm, scale=scene.scale, conf=scene.conf,
+                links=scene.links.astype(np.int32)).items()}
+    dview = core.tsr_samples_view(n, scene.k, dev["pos"].data_ptr(), dev["nrm"].data_ptr(), dev["scale"].data_ptr(),
+                                  dev["conf"].data_ptr(), dev["links"].data_ptr())
+
+    def device_step():
+        tree = ctypes.c_void_p()
+        core._check(core.lib.tsr_tree_build_device(ctypes.byref(dview), ctypes.byref(params), sptr,
+                                                   ctypes.byref(tree)))
+        occ = ctypes.c_void_p()
+        core._check(core.lib.tsr_occupancy_compute(tree, ctypes.byref(cams.view()), ctypes.byref(params), 0, sptr,
+                                                   ctypes.byref(occ)))
+        mesh = ctypes.c_void_p()
+        core._check(core.lib.tsr_dmc_extract(tree, occ, sptr, ctypes.byref(mesh)))
+        tc = core.tsr_tree_counts()
+        core._check(core.lib.tsr_tree_get_counts(tree, ctypes.byref(tc)))
+        mc = core.tsr_mesh_counts()
+        core._check(core.lib.tsr_mesh_get_counts(mesh, ctypes.byref(mc)))
+        tms = np.zeros(8, np.float32)
+        oms = np.zeros(8, np.float32)
+        core.lib.tsr_tree_stage_ms(tree, core._ptr(tms), 8)
+        core.lib.tsr_occupancy_stage_ms(occ, core._ptr(oms), 8)
+        core.lib.tsr_mesh_free(mesh)
+        core.lib.tsr_occupancy_free(occ)
+        core.lib.tsr_tree_free(tree)
+        return tc, mc, tms, oms
+
+    # ---- host buffers (pinned) for the e2e leg
+    def pinned(a):
+        t = torch.empty(a.shape, dtype=torch.from_numpy(a[:1]).dtype, pin_memory=True)
+        t.numpy()[...] = a
+        return t
+
+    host = {k: pinned(np.ascontiguousarray(v)) for k, v in
+            dict(pos=scene.pos, nrm=scene.nrm, scale=scene.scale, conf=scene.conf,
+                 links=scene.links.astype(np.int32)).items()}
+
+    def e2e_step():
+        # the samples stay in the caller's pinned buffers; the tree keeps its
+        # reordered copy in HBM (reorder_samples=False), the mesh comes back
+        s = core.Samples(host["pos"].numpy(), host["nrm"].numpy(), host["scale"].numpy(), host["conf"].numpy(),
+                         host["links"].numpy().view(np.uint32))
+        tree = core.Tree(s, params, stream=stream, reorder_samples=False)
+        occ = core.Occupancy(tree, cams, params, stream=stream)
+        mesh = occ.extractCrust(stream=stream)
+        return tree, mesh
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        device_step()
+    # ---- timed: value (device-resident inputs)
+    clocks = Clocks(local)
+    clocks.start()
+    barrier()
+    l0 = core.kernel_launches()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    stage_sum = np.zeros(16)
+    for i in range(args.steps):
+        ev[i][0].record(stream)
+        tc, mc, tms, oms = device_step()
+        ev[i][1].record(stream)
+        stage_sum += np.concatenate([tms, oms])
+    barrier()
+    launches = core.kernel_launches() - l0
+    clk = clocks.stop()
+    t_value = sum(a.elapsed_time(b) for a, b in ev) / 1e3
+    t_value = max_over_ranks(t_value)
+
+    # ---- timed: e2e through the public API from pinned host buffers
+    for _ in range(max(1, args.warmup // 2)):
+        e2e_step()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        tree, mesh = e2e_step()
+    barrier()
+    t_e2e = max_over_ranks(time.perf_counter() - t0)
+    h2d = n * (24 + 24 + 8 + 8 + 4 * scene.k) + scene.cams.nbytes
+    d2h = mesh.cases.nbytes + mesh.positions.nbytes + mesh.scales.nbytes + mesh.edge_keys.nbytes + \
+        mesh.triangles.nbytes
+
+    # ---- roofline of the dominant kernel (per-launch algorithmic bytes / event time)
+    stage_ms = stage_sum / args.steps
+    names = ["tree.containment", "tree.sampling", "tree.balance", "tree.relayout", "tree.neighbors",
+             "tree.dual_cells", "", "", "occ.sampleness", "occ.flags", "occ.emptiness", "occ.priors", "occ.finalize",
+             "", "", ""]
+    stages = {nm: float(v) for nm, v in zip(names, stage_ms) if nm}
+    K = scene.k
+    Nn, Nl = tc.nodes, tc.leaves
+    per_pass = n * (32 + 4 * K) + Nn * 8 + Nl * 16       # per cone pass
+    alg = {"occ.sampleness": per_pass, "occ.emptiness": per_pass, "occ.priors": Nl * (16 + 8),
+           "occ.finalize": Nl * (32 + 8)}
+    dom = max(alg, key=lambda k: stages[k])
+    hbm, src = peaks()
+    achieved = alg[dom] / (stages[dom] / 1e3) / 1e9
+    total_ms = sum(stages.values())
+
+    world_samples = n * world
+    line = {
+        "metric": METRIC, "value": world_samples * args.steps / t_value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_value / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": desc, "samples": n, "cameras": int(scene.cams.shape[0]), "k": K,
+                   "mode": "plain FP32 field (compensated sums), FP64 topology",
+                   "l2": "inputs %d MB > 126 MB L2; all buffers re-allocated each step" % (h2d // 2**20),
+                   "parallelism": "replicas" if world > 1 else "single GPU",
+                   "nodes": Nn, "leaves": Nl, "dual_cells": tc.dual_cells, "triangles": mc.triangles},
+        "e2e": {"value": world_samples * args.steps / t_e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": int(launches),
+        "stage_ms": {k: round(v, 3) for k, v in stages.items()},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm,
+                     "unit": "GB/s", "frac": achieved / hbm, "peak_source": src + " (MEASURED_PEAKS.json hbm_gbs)",
+                     "algorithmic_bytes": int(alg[dom]), "kernel_ms": stages[dom],
+                     "share_of_step": stages[dom] / total_ms if total_ms else None, "traffic": None},
+        "clocks": clk,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        cs = cpu_scene(args.workload)
+        tcpu = run_oracle_once(cs, threads)
+        line["cpu_baseline"] = {"value": cs.n / tcpu, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": "FP64 oracle full pipeline on the same geometry and cameras at %d samples"
+                                % cs.n}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="csg4m", choices=["csg4m", "sphere", "heldout16m"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        our_arm(args)
+
+
+if __name__ == "__main__":
+    main()

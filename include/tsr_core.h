@@ -118,12 +118,20 @@ TSR_API const char *tsr_version(void);
 
 TSR_API tsr_status tsr_tree_build(const tsr_samples_view *samples, const tsr_params *params,
                           void *cuda_stream, tsr_tree **out_tree);
+/* Same as tsr_tree_build with every pointer of `samples` in DEVICE memory
+ * (for callers whose samples already live in HBM). */
+TSR_API tsr_status tsr_tree_build_device(const tsr_samples_view *samples, const tsr_params *params,
+                                         void *cuda_stream, tsr_tree **out_tree);
 TSR_API void tsr_tree_free(tsr_tree *tree);
 TSR_API tsr_status tsr_tree_get_counts(const tsr_tree *tree, tsr_tree_counts *out);
 TSR_API tsr_status tsr_tree_root_scope(const tsr_tree *tree, double min_xyz_size[4]);
 /* Node arrays after the reference's reorder; any pointer may be NULL. */
 TSR_API tsr_status tsr_tree_copy_nodes(const tsr_tree *tree, uint32_t *children, uint32_t *parents,
                                uint32_t *sample_counts, uint32_t *sample_starts);
+/* The samples in tree order (Samples::reorder, Samples.cpp:825-835), into
+ * HOST arrays laid out like tsr_samples_view; any pointer may be NULL. */
+TSR_API tsr_status tsr_tree_copy_samples(const tsr_tree *tree, double *positions, double *normals,
+                                         double *scales, double *confidences, uint32_t *camera_links);
 /* target_indices[old sample index] = new sample index (Nodes.cpp:625-626). */
 TSR_API tsr_status tsr_tree_copy_permutation(const tsr_tree *tree, uint32_t *target_indices);
 /* scopes: 4 doubles per leaf (min x, y, z, size); node_index per leaf;
@@ -149,6 +157,10 @@ TSR_API tsr_status tsr_mesh_get_counts(const tsr_mesh *mesh, tsr_mesh_counts *ou
  * uint32 per triangle.  Any pointer may be NULL. */
 TSR_API tsr_status tsr_mesh_copy(const tsr_mesh *mesh, uint8_t *cases, double *positions, double *scales,
                          uint32_t *edge_keys, uint32_t *triangles);
+
+/* Number of this library's kernel launches so far in the process
+ * (instrumentation; no counterpart in the reference). */
+TSR_API unsigned long long tsr_kernel_launches(void);
 
 /* Wall-clock-free stage timing: CUDA-event milliseconds of the last call on
  * this handle, per stage (see tsr_stage names in the implementation). */

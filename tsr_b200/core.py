@@ -62,6 +62,9 @@ _sig = {
     "tsr_last_error_message": (ctypes.c_char_p, []),
     "tsr_version": (ctypes.c_char_p, []),
     "tsr_tree_build": (ctypes.c_int, [_P, _P, _P, _P]),
+    "tsr_tree_build_device": (ctypes.c_int, [_P, _P, _P, _P]),
+    "tsr_tree_copy_samples": (ctypes.c_int, [_P, _P, _P, _P, _P, _P]),
+    "tsr_kernel_launches": (ctypes.c_ulonglong, []),
     "tsr_tree_free": (None, [_P]),
     "tsr_tree_get_counts": (ctypes.c_int, [_P, _P]),
     "tsr_tree_root_scope": (ctypes.c_int, [_P, _P]),
@@ -143,7 +146,8 @@ class Samples:
 
     @classmethod
     def from_scene(cls, scene):
-        return cls(scene.pos, scene.nrm, scene.scale, scene.conf, scene.links)
+        """Copies the scene's arrays (a Tree reorders its Samples in place)."""
+        return cls(scene.pos.copy(), scene.nrm.copy(), scene.scale.copy(), scene.conf.copy(), scene.links.copy())
 
     @property
     def count(self):
@@ -244,7 +248,11 @@ class Tree:
         self.counts = {k: int(getattr(c, k)) for k, _ in tsr_tree_counts._fields_}
         self.sample_count = samples.count
         if reorder_samples:
-            samples.reorder(self.getPermutation())
+            # the reference reorders Samples in place (Nodes.cpp:630); copy the
+            # device-side reordered arrays back instead of permuting on the host
+            _check(lib.tsr_tree_copy_samples(self._h, _ptr(samples.positions), _ptr(samples.normals),
+                                             _ptr(samples.scales), _ptr(samples.confidences),
+                                             _ptr(samples.camera_links)))
         self._nodes = self._leaves = self._cells = None
 
     def __del__(self):
@@ -414,3 +422,8 @@ class DualMarchingCells:
 
 def version():
     return lib.tsr_version().decode()
+
+
+def kernel_launches():
+    """This library's kernel launches so far in the process."""
+    return int(lib.tsr_kernel_launches())

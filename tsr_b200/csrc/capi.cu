@@ -3,6 +3,7 @@
 // Each call validates its arguments, runs on the caller's stream, converts
 // internal failures into a tsr_status and keeps the message for
 // tsr_last_error_message() (the reference throws FailureHandling::Exception).
+#include <atomic>
 #include <cstring>
 #include <new>
 #include <string>
@@ -12,6 +13,9 @@
 namespace tsr {
 
 static thread_local std::string g_last_error;
+static std::atomic<unsigned long long> g_launches{0};
+
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 void fail(tsr_status st, const std::string &msg) { throw Error{st, msg}; }
 
@@ -70,8 +74,8 @@ const char *tsr_last_error_message(void) { return g_last_error.c_str(); }
 
 const char *tsr_version(void) { return "tsr_b200 core 0.1 (sm_100a)"; }
 
-tsr_status tsr_tree_build(const tsr_samples_view *samples, const tsr_params *params, void *cuda_stream,
-                          tsr_tree **out_tree) {
+static tsr_status tree_build_impl(const tsr_samples_view *samples, const tsr_params *params, void *cuda_stream,
+                                  tsr_tree **out_tree, bool on_device) {
     if (out_tree) *out_tree = nullptr;
     return guarded([&] {
         if (!samples || !out_tree) fail(TSR_ERR_INVALID_ARG, "null argument");
@@ -82,9 +86,10 @@ tsr_status tsr_tree_build(const tsr_samples_view *samples, const tsr_params *par
             fail(TSR_ERR_INVALID_ARG, "null sample array");
         if ((uint64_t)samples->count * samples->cams_per_sample >= 0xFFFFFFFFull)
             fail(TSR_ERR_OVERFLOW_U32, "link count must stay below 2^32 - 1 (Samples.h:395-402)");
-        for (uint32_t i = 0; i < samples->count; ++i)
-            if (!(samples->scales[i] > 0.0))   // Samples.cpp:280-288
-                fail(TSR_ERR_INVALID_ARG, "invalid (non-positive) sample scale at index " + std::to_string(i));
+        if (!on_device)
+            for (uint32_t i = 0; i < samples->count; ++i)
+                if (!(samples->scales[i] > 0.0))   // Samples.cpp:280-288
+                    fail(TSR_ERR_INVALID_ARG, "invalid (non-positive) sample scale at index " + std::to_string(i));
         tsr_params p;
         tsr_params_default(&p);
         if (params) p = *params;
@@ -93,7 +98,7 @@ tsr_status tsr_tree_build(const tsr_samples_view *samples, const tsr_params *par
         t->stream = (cudaStream_t)cuda_stream;
         t->params = p;
         try {
-            build_tree(*t, *samples);
+            build_tree(*t, *samples, on_device);
         } catch (...) {
             delete t;
             throw;
@@ -101,6 +106,18 @@ tsr_status tsr_tree_build(const tsr_samples_view *samples, const tsr_params *par
         *out_tree = t;
     });
 }
+
+tsr_status tsr_tree_build(const tsr_samples_view *samples, const tsr_params *params, void *cuda_stream,
+                          tsr_tree **out_tree) {
+    return tree_build_impl(samples, params, cuda_stream, out_tree, false);
+}
+
+tsr_status tsr_tree_build_device(const tsr_samples_view *samples, const tsr_params *params, void *cuda_stream,
+                                 tsr_tree **out_tree) {
+    return tree_build_impl(samples, params, cuda_stream, out_tree, true);
+}
+
+unsigned long long tsr_kernel_launches(void) { return g_launches.load(std::memory_order_relaxed); }
 
 void tsr_tree_free(tsr_tree *tree) { delete tree; }
 
@@ -132,6 +149,19 @@ tsr_status tsr_tree_copy_nodes(const tsr_tree *t, uint32_t *children, uint32_t *
         to_host(t->parents, t->n_nodes, parents, t->stream);
         to_host(t->counts, t->n_nodes, sample_counts, t->stream);
         to_host(t->starts, t->n_nodes, sample_starts, t->stream);
+        TSR_CUDA(cudaStreamSynchronize(t->stream));
+    });
+}
+
+tsr_status tsr_tree_copy_samples(const tsr_tree *t, double *positions, double *normals, double *scales,
+                                 double *confidences, uint32_t *camera_links) {
+    return guarded([&] {
+        if (!t) fail(TSR_ERR_INVALID_ARG, "null tree");
+        to_host(t->pos, t->n_samples, positions, t->stream);
+        to_host(t->nrm, t->n_samples, normals, t->stream);
+        to_host(t->scale, t->n_samples, scales, t->stream);
+        to_host(t->conf, t->n_samples, confidences, t->stream);
+        to_host(t->links, (size_t)t->n_samples * t->k, camera_links, t->stream);
         TSR_CUDA(cudaStreamSynchronize(t->stream));
     });
 }

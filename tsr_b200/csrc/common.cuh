@@ -29,6 +29,7 @@ struct Error {
 };
 
 [[noreturn]] void fail(tsr_status st, const std::string &msg);
+void note_launch();   // counts this library's kernel launches (instrumentation)
 void check_cuda(cudaError_t e, const char *what);
 #define TSR_CUDA(call) ::tsr::check_cuda((call), #call)
 

@@ -174,7 +174,7 @@ void extract_dmc(const tsr_tree &t, const tsr_occupancy &o, tsr_mesh &m) {
     DBuf<uint32_t> ntri(nc + 1, st), toff(nc + 1, st), active(1, st);
     active.zero();
     TSR_CUDA(cudaMemsetAsync(ntri.p + nc, 0, 4, st));
-    if (nc) k_classify<<<grid_for(nc, BLK), BLK, 0, st>>>(nc, t.cells.p, o.occ.p, m.cases.p, ntri.p, active.p);
+    if (nc) k_classify<<<grid_for(nc, BLK), BLK, 0, st>>>(nc, t.cells.p, o.occ.p, m.cases.p, ntri.p, active.p); ::tsr::note_launch();
     exscan(ntri.p, toff.p, nc + 1, st);
     uint32_t ntr = read_scalar(toff.p + nc, st);
     m.n_active = read_scalar(active.p, st);
@@ -189,10 +189,10 @@ void extract_dmc(const tsr_tree &t, const tsr_occupancy &o, tsr_mesh &m) {
     }
     DBuf<uint64_t> keys(mc, st), skeys(mc, st);
     DBuf<uint32_t> vals(mc, st), svals(mc, st), ends(2ull * mc, st);
-    k_emit<<<grid_for(nc, BLK), BLK, 0, st>>>(nc, t.cells.p, o.occ.p, toff.p, keys.p, vals.p, ends.p);
+    k_emit<<<grid_for(nc, BLK), BLK, 0, st>>>(nc, t.cells.p, o.occ.p, toff.p, keys.p, vals.p, ends.p); ::tsr::note_launch();
     sortp(keys.p, skeys.p, vals.p, svals.p, mc, st);
     DBuf<uint32_t> head(mc, st), segid(mc, st), first(mc, st);
-    k_heads<<<grid_for(mc, BLK), BLK, 0, st>>>(mc, skeys.p, svals.p, head.p, first.p);
+    k_heads<<<grid_for(mc, BLK), BLK, 0, st>>>(mc, skeys.p, svals.p, head.p, first.p); ::tsr::note_launch();
     {
         size_t tmp = 0;
         TSR_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tmp, head.p, segid.p, mc, st));
@@ -202,15 +202,15 @@ void extract_dmc(const tsr_tree &t, const tsr_occupancy &o, tsr_mesh &m) {
     uint32_t nv = read_scalar(segid.p + mc - 1, st);
     m.n_verts = nv;
     DBuf<uint32_t> seg_first(nv, st), seg_iota(nv, st), sfirst(nv, st), order(nv, st), vert_of_seg(nv, st);
-    k_seg_first<<<grid_for(mc, BLK), BLK, 0, st>>>(mc, head.p, segid.p, svals.p, seg_first.p, seg_iota.p);
+    k_seg_first<<<grid_for(mc, BLK), BLK, 0, st>>>(mc, head.p, segid.p, svals.p, seg_first.p, seg_iota.p); ::tsr::note_launch();
     sortp(seg_first.p, sfirst.p, seg_iota.p, order.p, nv, st);
-    k_rank<<<grid_for(nv, BLK), BLK, 0, st>>>(nv, order.p, vert_of_seg.p);
-    k_tris<<<grid_for(mc, BLK), BLK, 0, st>>>(mc, svals.p, segid.p, vert_of_seg.p, m.tris.p);
+    k_rank<<<grid_for(nv, BLK), BLK, 0, st>>>(nv, order.p, vert_of_seg.p); ::tsr::note_launch();
+    k_tris<<<grid_for(mc, BLK), BLK, 0, st>>>(mc, svals.p, segid.p, vert_of_seg.p, m.tris.p); ::tsr::note_launch();
     m.vpos.alloc(3ull * nv, st);
     m.vscale.alloc(nv, st);
     m.vkeys.alloc(2ull * nv, st);
     k_vertices<<<grid_for(nv, BLK), BLK, 0, st>>>(nv, order.p, seg_first.p, ends.p, t.leaf_min.p, t.leaf_node.p,
-                                                 t.depth.p, t.root_size, o.occ.p, m.vpos.p, m.vscale.p, m.vkeys.p);
+                                                 t.depth.p, t.root_size, o.occ.p, m.vpos.p, m.vscale.p, m.vkeys.p); ::tsr::note_launch();
     TSR_CUDA(cudaGetLastError());
 }
 

@@ -54,7 +54,7 @@ struct tsr_mesh {
 };
 
 namespace tsr {
-void build_tree(tsr_tree &t, const tsr_samples_view &sv);
+void build_tree(tsr_tree &t, const tsr_samples_view &sv, bool on_device);
 void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_params &p, int mode,
                        tsr_occupancy &o);
 void extract_dmc(const tsr_tree &t, const tsr_occupancy &o, tsr_mesh &m);

@@ -382,27 +382,27 @@ void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_
     unsigned grid = (unsigned)((nlinks + 127) / 128);
     if (grid == 0) grid = 1;
     k_cone_pass<SAMPLENESS><<<grid, 128, 0, st>>>(nlinks, in, tr, o.states.p, ssum, slen, cone_count.p, accepted.p + 1,
-                                                  err.p);
+                                                  err.p); ::tsr::note_launch();
     o.stage_ms[0] = timer.lap();
     // forwardAnyChildStateFlag(0, SAMPLENESS) before the EMPTINESS pass (Occupancy.cpp:141-142)
     for (int d = (int)t.level_start.size() - 2; d >= 0; --d) {
         uint32_t lo = t.level_start[d], hi = t.level_start[d + 1];
         k_forward_flag<<<grid_for(hi - lo, BLK), BLK, 0, st>>>(lo, hi, t.level_order.p, t.children.p, o.states.p,
-                                                              FLAG_SAMPLENESS);
+                                                              FLAG_SAMPLENESS); ::tsr::note_launch();
     }
     o.stage_ms[1] = timer.lap();
     k_cone_pass<EMPTINESS><<<grid, 128, 0, st>>>(nlinks, in, tr, o.states.p, esum, elen, cone_count.p, accepted.p,
-                                                 err.p);
+                                                 err.p); ::tsr::note_launch();
     o.stage_ms[2] = timer.lap();
     o.prior.alloc(nl, st);
     k_priors<<<grid_for(nl, 128), 128, 0, st>>>(nl, t.leaf_node.p, t.leaf_min.p, tr, o.states.p, elen, slen,
-                                               t.root_size, p.relative_radius_for_priors, o.prior.p, err.p);
+                                               t.root_size, p.relative_radius_for_priors, o.prior.p, err.p); ::tsr::note_launch();
     o.stage_ms[3] = timer.lap();
     o.cone_count = read_scalar(cone_count.p, st);
     o.e_sum.alloc(nl, st); o.s_sum.alloc(nl, st); o.e_len.alloc(nl, st); o.s_len.alloc(nl, st); o.occ.alloc(nl, st);
     k_finalize<<<grid_for(nl, BLK), BLK, 0, st>>>(nl, esum, ssum, elen, slen, o.prior.p, o.cone_count,
                                                  p.confidence_threshold, o.e_sum.p, o.s_sum.p, o.e_len.p, o.s_len.p,
-                                                 o.occ.p);
+                                                 o.occ.p); ::tsr::note_launch();
     o.stage_ms[4] = timer.lap();
     unsigned long long a[2];
     TSR_CUDA(cudaMemcpyAsync(a, accepted.p, 16, cudaMemcpyDeviceToHost, st));

@@ -849,7 +849,7 @@ struct EventTimer {
 }  // namespace
 
 // ====================================================================== API
-void build_tree(tsr_tree &t, const tsr_samples_view &sv) {
+void build_tree(tsr_tree &t, const tsr_samples_view &sv, bool on_device) {
     cudaStream_t st = t.stream;
     const uint32_t n = sv.count, k = sv.cams_per_sample;
     const double h_svo = t.params.max_relative_sampling_distance;
@@ -861,17 +861,18 @@ void build_tree(tsr_tree &t, const tsr_samples_view &sv) {
     DBuf<D3> pos(n, st), nrm(n, st);
     DBuf<double> scale(n, st), conf(n, st);
     DBuf<uint32_t> links((size_t)n * k, st);
-    TSR_CUDA(cudaMemcpyAsync(pos.p, sv.positions, (size_t)n * 24, cudaMemcpyHostToDevice, st));
-    TSR_CUDA(cudaMemcpyAsync(nrm.p, sv.normals, (size_t)n * 24, cudaMemcpyHostToDevice, st));
-    TSR_CUDA(cudaMemcpyAsync(scale.p, sv.scales, (size_t)n * 8, cudaMemcpyHostToDevice, st));
-    TSR_CUDA(cudaMemcpyAsync(conf.p, sv.confidences, (size_t)n * 8, cudaMemcpyHostToDevice, st));
-    TSR_CUDA(cudaMemcpyAsync(links.p, sv.camera_links, (size_t)n * k * 4, cudaMemcpyHostToDevice, st));
+    const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    TSR_CUDA(cudaMemcpyAsync(pos.p, sv.positions, (size_t)n * 24, kind, st));
+    TSR_CUDA(cudaMemcpyAsync(nrm.p, sv.normals, (size_t)n * 24, kind, st));
+    TSR_CUDA(cudaMemcpyAsync(scale.p, sv.scales, (size_t)n * 8, kind, st));
+    TSR_CUDA(cudaMemcpyAsync(conf.p, sv.confidences, (size_t)n * 8, kind, st));
+    TSR_CUDA(cudaMemcpyAsync(links.p, sv.camera_links, (size_t)n * k * 4, kind, st));
 
     // ---- root scope (Tree.cpp:70-101)
     {
         unsigned g = std::min<unsigned>(grid_for(n, BLK), 1024);
         DBuf<double> part((size_t)g * 6, st);
-        k_bounds<<<g, BLK, 0, st>>>(n, pos.p, scale.p, h_svo, part.p);
+        k_bounds<<<g, BLK, 0, st>>>(n, pos.p, scale.p, h_svo, part.p); ::tsr::note_launch();
         std::vector<double> h((size_t)g * 6);
         TSR_CUDA(cudaMemcpyAsync(h.data(), part.p, h.size() * 8, cudaMemcpyDeviceToHost, st));
         TSR_CUDA(cudaStreamSynchronize(st));
@@ -915,7 +916,7 @@ void build_tree(tsr_tree &t, const tsr_samples_view &sv) {
         uint32_t width = lvl_hi - lvl_lo;
         DBuf<uint32_t> need((size_t)S.cap + 1, st);
         TSR_CUDA(cudaMemsetAsync(need.p + lvl_lo, 0, ((size_t)width + 1) * 4, st));
-        k_contain_mark<<<grid_for(n, BLK), BLK, 0, st>>>(n, scale.p, h_svo, size_l, cur.p, container.p, need.p, S.cnt.p);
+        k_contain_mark<<<grid_for(n, BLK), BLK, 0, st>>>(n, scale.p, h_svo, size_l, cur.p, container.p, need.p, S.cnt.p); ::tsr::note_launch();
         DBuf<uint32_t> rank(width + 1, st);
         TSR_CUDA(cudaMemsetAsync(rank.p + width, 0, 4, st));
         exclusive_scan(need.p + lvl_lo, rank.p, width + 1, st);   // last entry = total
@@ -926,8 +927,8 @@ void build_tree(tsr_tree &t, const tsr_samples_view &sv) {
         S.ensure((uint64_t)S.count + 8ull * nneed);
         NV v = view(S);
         k_contain_alloc<<<grid_for(width, BLK), BLK, 0, st>>>(lvl_lo, lvl_hi, need.p, rank.p, v, base,
-                                                               size_at(root.size, level + 1));
-        k_contain_step<<<grid_for(n, BLK), BLK, 0, st>>>(n, pos.p, size_at(root.size, level + 1), cur.p, container.p, v);
+                                                               size_at(root.size, level + 1)); ::tsr::note_launch();
+        k_contain_step<<<grid_for(n, BLK), BLK, 0, st>>>(n, pos.p, size_at(root.size, level + 1), cur.p, container.p, v); ::tsr::note_launch();
         S.count += 8 * nneed;
         lvl_lo = base;
         lvl_hi = S.count;
@@ -941,7 +942,7 @@ void build_tree(tsr_tree &t, const tsr_samples_view &sv) {
         if ((uint64_t)n * 2 >= INVALID) fail(TSR_ERR_OVERFLOW_U32, "too many samples");
         uint32_t m = 2 * n;
         DBuf<uint32_t> keys(m, st), keys2(m, st);
-        k_keys_init<<<grid_for(m, BLK), BLK, 0, st>>>(m, keys.p);
+        k_keys_init<<<grid_for(m, BLK), BLK, 0, st>>>(m, keys.p); ::tsr::note_launch();
         DBuf<uint32_t> mark;
         mark.alloc(S.cap, st);
         mark.fill_bytes(0xFF);
@@ -956,24 +957,24 @@ void build_tree(tsr_tree &t, const tsr_samples_view &sv) {
             DBuf<uint32_t> witness(m, st), dleaf(m, st);
             unres.zero();
             k_sampling_eval<<<grid_for(m, 128), 128, 0, st>>>(m, keys.p, v, root, pos.p, nrm.p, scale.p, h_svo,
-                                                             status.p, witness.p, dleaf.p, derr.p);
+                                                             status.p, witness.p, dleaf.p, derr.p); ::tsr::note_launch();
             if (int e0 = read_scalar(derr.p, st))
                 fail(TSR_ERR_DEVICE_ASSERT, "sampling evaluation invariant broken (code " + std::to_string(e0) + ")");
             for (int it = 0;; ++it) {
                 if (it > 1000000) fail(TSR_ERR_TIMEOUT, "sampling conflict resolution did not converge");
                 changed.zero();
-                k_sampling_mark<<<grid_for(m, BLK), BLK, 0, st>>>(m, keys.p, status.p, unres.p, dleaf.p, mark.p);
+                k_sampling_mark<<<grid_for(m, BLK), BLK, 0, st>>>(m, keys.p, status.p, unres.p, dleaf.p, mark.p); ::tsr::note_launch();
                 k_sampling_conflict<<<grid_for(m, 128), 128, 0, st>>>(m, keys.p, v, root, pos.p, nrm.p, scale.p, h_svo,
                                                                      status.p, witness.p, dleaf.p, mark.p, unres.p,
-                                                                     changed.p, derr.p);
+                                                                     changed.p, derr.p); ::tsr::note_launch();
                 if (read_scalar(changed.p, st) == 0) break;
             }
-            k_count_writers<<<grid_for(m, BLK), BLK, 0, st>>>(m, status.p, unres.p, wcount.p);
+            k_count_writers<<<grid_for(m, BLK), BLK, 0, st>>>(m, status.p, unres.p, wcount.p); ::tsr::note_launch();
             // commit resolved writers
             DBuf<uint32_t> nsplit(m + 1, st), base(m + 1, st);
             TSR_CUDA(cudaMemsetAsync(nsplit.p + m, 0, 4, st));
             k_sampling_apply<<<grid_for(m, 128), 128, 0, st>>>(m, keys.p, status.p, unres.p, dleaf.p, v, root, pos.p,
-                                                              nrm.p, scale.p, h_svo, nsplit.p, nullptr, 0, 0, derr.p);
+                                                              nrm.p, scale.p, h_svo, nsplit.p, nullptr, 0, 0, derr.p); ::tsr::note_launch();
             exclusive_scan(nsplit.p, base.p, m + 1, st);
             uint32_t total = read_scalar(base.p + m, st);
             if (total) {
@@ -988,10 +989,10 @@ void build_tree(tsr_tree &t, const tsr_samples_view &sv) {
                 v = view(S);
                 k_sampling_apply<<<grid_for(m, 128), 128, 0, st>>>(m, keys.p, status.p, unres.p, dleaf.p, v, root,
                                                                   pos.p, nrm.p, scale.p, h_svo, nsplit.p, base.p,
-                                                                  S.count, 1, derr.p);
+                                                                  S.count, 1, derr.p); ::tsr::note_launch();
                 S.count += 8 * total;
             }
-            k_sampling_unmark<<<grid_for(m, BLK), BLK, 0, st>>>(m, dleaf.p, mark.p);
+            k_sampling_unmark<<<grid_for(m, BLK), BLK, 0, st>>>(m, dleaf.p, mark.p); ::tsr::note_launch();
             // next round: unresolved sides only
             uint32_t m2 = select_flagged(keys.p, unres.p, keys2.p, m, st);
             std::swap(keys, keys2);
@@ -1007,7 +1008,7 @@ void build_tree(tsr_tree &t, const tsr_samples_view &sv) {
     // ---- balancing rounds (Nodes.cpp:339-395)
     {
         DBuf<uint32_t> list(S.count, st);
-        k_iota<<<grid_for(S.count, BLK), BLK, 0, st>>>(S.count, list.p);
+        k_iota<<<grid_for(S.count, BLK), BLK, 0, st>>>(S.count, list.p); ::tsr::note_launch();
         uint32_t m = S.count;
         DBuf<uint32_t> split_flag(S.cap, st);
         split_flag.zero();
@@ -1018,7 +1019,7 @@ void build_tree(tsr_tree &t, const tsr_samples_view &sv) {
             DBuf<uint32_t> split_list(m * 6 < S.count ? m * 6 : S.count, st), again(m, st);
             counters.zero();
             k_balance_check<<<grid_for(m, 128), 128, 0, st>>>(m, list.p, v, root, split_flag.p, split_list.p,
-                                                             counters.p, again.p, counters.p + 1);
+                                                             counters.p, again.p, counters.p + 1); ::tsr::note_launch();
             uint32_t cnt[2];
             TSR_CUDA(cudaMemcpyAsync(cnt, counters.p, 8, cudaMemcpyDeviceToHost, st));
             TSR_CUDA(cudaStreamSynchronize(st));
@@ -1035,7 +1036,7 @@ void build_tree(tsr_tree &t, const tsr_samples_view &sv) {
             uint32_t m2 = 8 * cnt[0] + cnt[1];
             DBuf<uint32_t> next(m2, st);
             k_balance_split<<<grid_for(cnt[0], BLK), BLK, 0, st>>>(cnt[0], split_list.p, split_flag.p, v, root, S.count,
-                                                                  next.p, 0);
+                                                                  next.p, 0); ::tsr::note_launch();
             if (cnt[1]) TSR_CUDA(cudaMemcpyAsync(next.p + 8 * cnt[0], again.p, (size_t)cnt[1] * 4, cudaMemcpyDeviceToDevice, st));
             S.count += 8 * cnt[0];
             list = std::move(next);
@@ -1053,30 +1054,30 @@ void build_tree(tsr_tree &t, const tsr_samples_view &sv) {
     {
         DBuf<uint32_t> iota(nn, st), order(nn, st);
         DBuf<uint8_t> sdepth(nn, st);
-        k_iota<<<grid_for(nn, BLK), BLK, 0, st>>>(nn, iota.p);
+        k_iota<<<grid_for(nn, BLK), BLK, 0, st>>>(nn, iota.p); ::tsr::note_launch();
         sort_pairs(S.depth.p, sdepth.p, iota.p, order.p, nn, st, 8);
         uint8_t dmax = read_scalar(sdepth.p + nn - 1, st);
         max_depth = dmax;
         DBuf<uint32_t> lstart(dmax + 2, st);
-        k_level_bounds<<<grid_for(nn, BLK), BLK, 0, st>>>(nn, sdepth.p, lstart.p);
+        k_level_bounds<<<grid_for(nn, BLK), BLK, 0, st>>>(nn, sdepth.p, lstart.p); ::tsr::note_launch();
         std::vector<uint32_t> ls(dmax + 2);
         TSR_CUDA(cudaMemcpyAsync(ls.data(), lstart.p, (dmax + 2) * 4, cudaMemcpyDeviceToHost, st));
         TSR_CUDA(cudaStreamSynchronize(st));
         DBuf<uint32_t> desc(nn, st), nleaf(nn, st);
         for (int d = dmax; d >= 0; --d)
-            k_subtree<<<grid_for(ls[d + 1] - ls[d], BLK), BLK, 0, st>>>(ls[d], ls[d + 1], order.p, S.children.p, desc.p, nleaf.p);
+            k_subtree<<<grid_for(ls[d + 1] - ls[d], BLK), BLK, 0, st>>>(ls[d], ls[d + 1], order.p, S.children.p, desc.p, nleaf.p); ::tsr::note_launch();
         uint32_t zero = 0, one = 1;
         TSR_CUDA(cudaMemcpyAsync(new_idx.p, &zero, 4, cudaMemcpyHostToDevice, st));
         TSR_CUDA(cudaMemcpyAsync(block.p, &one, 4, cudaMemcpyHostToDevice, st));
         TSR_CUDA(cudaMemcpyAsync(leaf_start.p, &zero, 4, cudaMemcpyHostToDevice, st));
         for (uint32_t d = 0; d <= dmax; ++d)
             k_layout<<<grid_for(ls[d + 1] - ls[d], BLK), BLK, 0, st>>>(ls[d], ls[d + 1], order.p, S.children.p, desc.p,
-                                                                     nleaf.p, new_idx.p, block.p, leaf_start.p);
+                                                                     nleaf.p, new_idx.p, block.p, leaf_start.p); ::tsr::note_launch();
         t.n_leaves = read_scalar(nleaf.p + 0, st);
         // level lists in the final numbering, for bottom-up passes
         t.level_start.assign(ls.begin(), ls.end());
         t.level_order.alloc(nn, st);
-        k_map_order<<<grid_for(nn, BLK), BLK, 0, st>>>(nn, order.p, new_idx.p, t.level_order.p);
+        k_map_order<<<grid_for(nn, BLK), BLK, 0, st>>>(nn, order.p, new_idx.p, t.level_order.p); ::tsr::note_launch();
         TSR_CUDA(cudaStreamSynchronize(st));
     }
     t.max_depth = max_depth;
@@ -1085,18 +1086,18 @@ void build_tree(tsr_tree &t, const tsr_samples_view &sv) {
     t.leaf_min.alloc(t.n_leaves, st); t.leaf_node.alloc(t.n_leaves, st);
     k_scatter_nodes<<<grid_for(nn, BLK), BLK, 0, st>>>(nn, v, new_idx.p, block.p, leaf_start.p, t.children.p, t.parents.p,
                                                       t.counts.p, t.depth.p, t.nmin.p, t.node_to_leaf.p, t.leaf_min.p,
-                                                      t.leaf_node.p);
+                                                      t.leaf_node.p); ::tsr::note_launch();
     exclusive_scan(t.counts.p, t.starts.p, nn, st);
 
     // ---- sample reorder (Nodes.cpp:594-636, Samples.cpp:825-835)
     {
         DBuf<uint32_t> keys(n, st), vals(n, st), skeys(n, st), old_of_new(n, st);
-        k_sample_keys<<<grid_for(n, BLK), BLK, 0, st>>>(n, container.p, new_idx.p, keys.p, vals.p);
+        k_sample_keys<<<grid_for(n, BLK), BLK, 0, st>>>(n, container.p, new_idx.p, keys.p, vals.p); ::tsr::note_launch();
         sort_pairs(keys.p, skeys.p, vals.p, old_of_new.p, n, st);
         t.target.alloc(n, st); t.pos.alloc(n, st); t.nrm.alloc(n, st); t.scale.alloc(n, st); t.conf.alloc(n, st);
         t.links.alloc((size_t)n * k, st);
         k_permute_samples<<<grid_for(n, BLK), BLK, 0, st>>>(n, k, old_of_new.p, t.target.p, pos.p, nrm.p, scale.p, conf.p,
-                                                           links.p, t.pos.p, t.nrm.p, t.scale.p, t.conf.p, t.links.p);
+                                                           links.p, t.pos.p, t.nrm.p, t.scale.p, t.conf.p, t.links.p); ::tsr::note_launch();
     }
     t.stage_ms[3] = timer.lap();
 
@@ -1109,10 +1110,10 @@ void build_tree(tsr_tree &t, const tsr_samples_view &sv) {
         DBuf<uint32_t> dst(ne, st), rowc(nl + 1, st), flag(ne + 1, st), slot(ne + 1, st);
         rowc.zero();
         k_neighbor_events<<<grid_for(ne, 128), 128, 0, st>>>(nl, t.leaf_node.p, t.leaf_min.p, t.children.p, t.nmin.p,
-                                                            t.depth.p, t.node_to_leaf.p, root, dst.p, rowc.p);
+                                                            t.depth.p, t.node_to_leaf.p, root, dst.p, rowc.p); ::tsr::note_launch();
         t.nb_off.alloc(nl + 1, st);
         exclusive_scan(rowc.p, t.nb_off.p, nl + 1, st);
-        k_valid_flags<<<grid_for(ne, BLK), BLK, 0, st>>>(ne, dst.p, flag.p);
+        k_valid_flags<<<grid_for(ne, BLK), BLK, 0, st>>>(ne, dst.p, flag.p); ::tsr::note_launch();
         TSR_CUDA(cudaMemsetAsync(flag.p + ne, 0, 4, st));
         exclusive_scan(flag.p, slot.p, ne + 1, st);
         uint32_t nev = read_scalar(slot.p + ne, st);
@@ -1121,7 +1122,7 @@ void build_tree(tsr_tree &t, const tsr_samples_view &sv) {
         DBuf<uint64_t> keys(nent, st), skeys(nent, st);
         DBuf<uint32_t> vals(nent, st);
         t.nbs.alloc(nent, st);
-        k_neighbor_pairs<<<grid_for(ne, BLK), BLK, 0, st>>>(ne, dst.p, slot.p, keys.p, vals.p);
+        k_neighbor_pairs<<<grid_for(ne, BLK), BLK, 0, st>>>(ne, dst.p, slot.p, keys.p, vals.p); ::tsr::note_launch();
         if (nent) sort_pairs(keys.p, skeys.p, vals.p, t.nbs.p, (uint32_t)nent, st);
     }
     t.stage_ms[4] = timer.lap();
@@ -1152,7 +1153,7 @@ void build_tree(tsr_tree &t, const tsr_samples_view &sv) {
             TSR_CUDA(cudaMemsetAsync(cf.p + nf, 0, 4, st));
             TSR_CUDA(cudaMemsetAsync(cc.p + nf, 0, 4, st));
             k_frames_count<<<grid_for(nf, 128), 128, 0, st>>>(nf, cur_f.type.p, cur_f.nodes.p, level, t.children.p,
-                                                             t.node_to_leaf.p, cf.p, cc.p);
+                                                             t.node_to_leaf.p, cf.p, cc.p); ::tsr::note_launch();
             exclusive_scan(cf.p, of.p, nf + 1, st);
             exclusive_scan(cc.p, oc.p, nf + 1, st);
             uint32_t tot[2];
@@ -1177,7 +1178,7 @@ void build_tree(tsr_tree &t, const tsr_samples_view &sv) {
             k_frames_write<<<grid_for(nf, 128), 128, 0, st>>>(nf, cur_f.type.p, cur_f.nodes.p, cur_f.khi.p, cur_f.klo.p,
                                                              level, t.children.p, t.node_to_leaf.p, of.p, oc.p, ncells,
                                                              nx.type.p, nx.nodes.p, nx.khi.p, nx.klo.p, all_cells.p,
-                                                             all_hi.p, all_lo.p);
+                                                             all_hi.p, all_lo.p); ::tsr::note_launch();
             ncells += tot[1];
             cur_f = std::move(nx);
             nf = tot[0];
@@ -1187,13 +1188,13 @@ void build_tree(tsr_tree &t, const tsr_samples_view &sv) {
         if (ncells) {
             DBuf<uint32_t> idx(ncells, st), idx2(ncells, st), idx3(ncells, st);
             DBuf<uint64_t> k2(ncells, st), k3(ncells, st);
-            k_iota<<<grid_for(ncells, BLK), BLK, 0, st>>>(ncells, idx.p);
+            k_iota<<<grid_for(ncells, BLK), BLK, 0, st>>>(ncells, idx.p); ::tsr::note_launch();
             // LSD: stable sort by the low word, then by the high word
             sort_pairs(all_lo.p, k2.p, idx.p, idx2.p, ncells, st);
             DBuf<uint64_t> hi_sorted(ncells, st);
-            k_gather_u64<<<grid_for(ncells, BLK), BLK, 0, st>>>(ncells, idx2.p, all_hi.p, hi_sorted.p);
+            k_gather_u64<<<grid_for(ncells, BLK), BLK, 0, st>>>(ncells, idx2.p, all_hi.p, hi_sorted.p); ::tsr::note_launch();
             sort_pairs(hi_sorted.p, k3.p, idx2.p, idx3.p, ncells, st);
-            k_gather_cells<<<grid_for(ncells, BLK), BLK, 0, st>>>(ncells, idx3.p, all_cells.p, t.cells.p);
+            k_gather_cells<<<grid_for(ncells, BLK), BLK, 0, st>>>(ncells, idx3.p, all_cells.p, t.cells.p); ::tsr::note_launch();
         }
     }
     t.stage_ms[5] = timer.lap();

@@ -282,7 +282,7 @@ def _random_cams(rng, n, dmin, dmax):
     return v * rng.uniform(dmin, dmax, n)[:, None]
 
 
-def csg_scene(seed=0, n_target=4_000_000, width=640, height=480, f=500.0, n_cams=120):
+def csg_scene(seed=0, n_target=4_000_000, width=1024, height=768, f=500.0, n_cams=120):
     """2 mm plate, cylinder r = 0.3, torus R = 0.5 / r = 0.1 in the box [-1, 1]^3."""
     rng = np.random.default_rng(seed)
     prims = [Box([-0.9, -0.9, -0.601], [0.9, 0.9, -0.599]),
