@@ -26,9 +26,28 @@ void check_cuda(cudaError_t e, const char *what) {
     fail(st, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+// The build allocates and frees large stream-ordered buffers many times per
+// call; keep freed memory in the current device's default pool instead of
+// unmapping it at every synchronization (once per device).
+static void keep_pool_memory() {
+    static std::atomic<uint64_t> done_mask{0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev >= 64) { (void)cudaGetLastError(); return; }
+    uint64_t bit = 1ull << dev;
+    if (done_mask.load() & bit) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t threshold = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+    }
+    (void)cudaGetLastError();
+    done_mask.fetch_or(bit);
+}
+
 template <class F>
 static tsr_status guarded(F &&f) {
     try {
+        keep_pool_memory();
         f();
         return TSR_OK;
     } catch (const Error &e) {

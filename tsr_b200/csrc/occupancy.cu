@@ -197,20 +197,48 @@ __global__ void __launch_bounds__(128) k_cone_pass(uint64_t nlinks, LinkIn in, T
             if ((states[node] & leaf_flag) == 0) atomicOr(&states[node], leaf_flag);
             ++acc;
         };
-        F3 rmin = rel(tr.nmin[0], p);
-        if (ignored(0, rmin, root_size_f)) break;
-        if (tr.children[0] == INVALID) { visit_leaf(0, rmin, root_size_f); break; }
+        // Start at the deepest node that contains the cut cone's bounding box
+        // (the capsule of radius R around the cut axis): every ancestor then
+        // contains the whole cone, so none of them can be pruned, and no leaf
+        // outside it can hold a point of the cone.
+        F3 p0 = c.end + c.axis * c.t_start_e;
+        F3 lo = f3(fminf(p0.x, c.end.x) - c.radius, fminf(p0.y, c.end.y) - c.radius, fminf(p0.z, c.end.z) - c.radius);
+        F3 hi = f3(fmaxf(p0.x, c.end.x) + c.radius, fmaxf(p0.y, c.end.y) + c.radius, fmaxf(p0.z, c.end.z) + c.radius);
+        uint32_t start = 0, base = 0;
+        F3 smin = rel(tr.nmin[0], p);
+        float ssize = root_size_f;
+        while (tr.children[start] != INVALID && base + 1 <= max_depth) {
+            float cs = 0.5f * ssize;
+            float margin = 1e-5f * ssize;
+            F3 ctr = smin + f3(cs, cs, cs);
+            uint32_t digit = 0;
+            bool inside = true;
+            const float l3[3] = {lo.x, lo.y, lo.z}, h3[3] = {hi.x, hi.y, hi.z}, c3[3] = {ctr.x, ctr.y, ctr.z};
+            for (int a = 0; a < 3; ++a) {
+                if (h3[a] < c3[a] - margin) continue;
+                if (l3[a] > c3[a] + margin) { digit |= 1u << a; continue; }
+                inside = false;
+            }
+            if (!inside) break;
+            start = tr.children[start] + digit;
+            smin = rel(tr.nmin[start], p);
+            ssize = cs;
+            ++base;
+        }
+        if (ignored(start, smin, ssize)) break;
+        if (tr.children[start] == INVALID) { visit_leaf(start, smin, ssize); break; }
+        if (base + 1 > max_depth) break;
         uint32_t st_node[MAX_TREE_DEPTH];
         uint8_t st_next[MAX_TREE_DEPTH];
         int sp = 1;
-        st_node[0] = 0;
+        st_node[0] = start;
         st_next[0] = 0;
         while (sp > 0) {
             int t = sp - 1;
             if (st_next[t] == 8) { --sp; continue; }
             uint32_t ci = st_next[t]++;
             uint32_t idx = tr.children[st_node[t]] + ci;
-            uint32_t d = (uint32_t)t + 1;   // depth of the child
+            uint32_t d = base + (uint32_t)t + 1;   // depth of the child
             float size = ldexpf(root_size_f, -(int)d);
             F3 bmin = rel(tr.nmin[idx], p);
             if (ignored(idx, bmin, size)) continue;
@@ -251,12 +279,59 @@ __global__ void k_forward_flag(uint32_t lo, uint32_t hi, const uint32_t *order, 
 
 __device__ inline double comp_value(float2 v) { return (double)v.x + (double)v.y; }
 
+// Cumulative prior sums per node: psum[node * PK + k] = sum of (emptiness,
+// sampleness) cone lengths over SAMPLENESS-flagged leaves of the node's
+// subtree at most k levels below the node.  Built bottom-up, one level per
+// launch.
+constexpr int PK = 8;
+
+__global__ void k_prior_sums(uint32_t lo, uint32_t hi, const uint32_t *order, const uint32_t *children,
+                             const uint32_t *node_to_leaf, const uint32_t *states, const float2 *elen,
+                             const float2 *slen, double2 *psum) {
+    uint32_t i = lo + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= hi) return;
+    uint32_t n = order[i];
+    uint32_t c0 = children[n];
+    double2 *dst = psum + (size_t)n * PK;
+    if (c0 == INVALID) {
+        double2 v = make_double2(0.0, 0.0);
+        if (states[n] & FLAG_SAMPLENESS) {
+            uint32_t l = node_to_leaf[n];
+            v = make_double2(comp_value(elen[l]), comp_value(slen[l]));
+        }
+        for (int k = 0; k < PK; ++k) dst[k] = v;
+        return;
+    }
+    dst[0] = make_double2(0.0, 0.0);
+    for (int k = 1; k < PK; ++k) {
+        double e = 0.0, s = 0.0;
+        for (uint32_t c = 0; c < 8; ++c) {
+            double2 v = psum[(size_t)(c0 + c) * PK + k - 1];
+            e += v.x;
+            s += v.y;
+        }
+        dst[k] = make_double2(e, s);
+    }
+}
+
+// Box entirely inside the sphere, with a strict relative margin so that every
+// leaf below certainly passes the closed sphere/box test.
+__device__ inline bool box_inside_sphere(const D3 &mn, double sz, const D3 &c, double r) {
+    double dx = fmax(fabs(c.x - mn.x), fabs(mn.x + sz - c.x));
+    double dy = fmax(fabs(c.y - mn.y), fabs(mn.y + sz - c.y));
+    double dz = fmax(fabs(c.z - mn.z), fabs(mn.z + sz - c.z));
+    return dx * dx + dy * dy + dz * dz <= r * r * (1.0 - 1e-9);
+}
+
 // Occupancy::computePriors (Occupancy.cpp:530-568) with a
-// SphereNodeStatesChecker (SphereNodeStatesChecker.cpp:28-36).
-__global__ void __launch_bounds__(128) k_priors(uint32_t nl, const uint32_t *leaf_node, const D3 *leaf_min,
-                                                TreeIn tr, const uint32_t *states, const float2 *elen,
-                                                const float2 *slen, double root_size, double rel_radius,
-                                                double *prior, int *err) {
+// SphereNodeStatesChecker (SphereNodeStatesChecker.cpp:28-36).  The set of
+// summed leaves is the reference's: SAMPLENESS-flagged leaves at most three
+// levels below the query leaf whose box meets the sphere (the exact FP64
+// test); subtrees wholly inside the sphere are added from psum.
+__global__ void __launch_bounds__(128) k_priors_h(uint32_t nl, const uint32_t *leaf_node, const D3 *leaf_min,
+                                                  TreeIn tr, const uint32_t *states, const float2 *elen,
+                                                  const float2 *slen, const double2 *psum, double root_size,
+                                                  double rel_radius, double *prior, int *err) {
     uint32_t l = blockIdx.x * blockDim.x + threadIdx.x;
     if (l >= nl) return;
     uint32_t node = leaf_node[l];
@@ -268,19 +343,29 @@ __global__ void __launch_bounds__(128) k_priors(uint32_t nl, const uint32_t *lea
     double radius = dmul(size, rel_radius);
     uint32_t max_depth = ld + MAX_DEPTH_DIFFERENCE;
     double eL = 0.0, sL = 0.0;
-    auto ignored = [&](uint32_t n, double sz, uint32_t depth) -> bool {
-        if ((states[n] & FLAG_SAMPLENESS) == 0) return true;
-        if (depth > max_depth) return true;
-        D3 bmn = tr.nmin[n];
+    // returns 0 = ignored, 1 = add subtree sum, 2 = visit / descend
+    auto classify = [&](uint32_t n, const D3 &bmn, double sz, uint32_t depth) -> int {
+        if ((states[n] & FLAG_SAMPLENESS) == 0) return 0;
+        if (depth > max_depth) return 0;
         D3 bmx{dadd(bmn.x, sz), dadd(bmn.y, sz), dadd(bmn.z, sz)};
-        return !aabb_sphere(bmn, bmx, center, radius);
+        if (!aabb_sphere(bmn, bmx, center, radius)) return 0;
+        if (max_depth - depth < (uint32_t)PK && box_inside_sphere(bmn, sz, center, radius)) return 1;
+        return 2;
+    };
+    auto add_sum = [&](uint32_t n, uint32_t depth) {
+        double2 v = psum[(size_t)n * PK + (max_depth - depth)];
+        eL += v.x;
+        sL += v.y;
     };
     auto visit = [&](uint32_t n) {
         uint32_t leaf = tr.node_to_leaf[n];
         eL += comp_value(elen[leaf]);
         sL += comp_value(slen[leaf]);
     };
-    if (!ignored(0, root_size, 0)) {
+    int rc = classify(0, tr.nmin[0], root_size, 0);
+    if (rc == 1) {
+        add_sum(0, 0);
+    } else if (rc == 2) {
         if (tr.children[0] == INVALID) {
             visit(0);
         } else {
@@ -296,7 +381,9 @@ __global__ void __launch_bounds__(128) k_priors(uint32_t nl, const uint32_t *lea
                 uint32_t idx = tr.children[st_node[t]] + ci;
                 uint32_t d = (uint32_t)t + 1;
                 double sz = size_at(root_size, d);
-                if (ignored(idx, sz, d)) continue;
+                int c = classify(idx, tr.nmin[idx], sz, d);
+                if (c == 0) continue;
+                if (c == 1) { add_sum(idx, d); continue; }
                 if (tr.children[idx] == INVALID) { visit(idx); continue; }
                 if (d + 1 > max_depth) continue;
                 if (sp >= MAX_TREE_DEPTH) { atomicExch(err, 2); break; }
@@ -395,8 +482,17 @@ void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_
                                                  err.p); ::tsr::note_launch();
     o.stage_ms[2] = timer.lap();
     o.prior.alloc(nl, st);
-    k_priors<<<grid_for(nl, 128), 128, 0, st>>>(nl, t.leaf_node.p, t.leaf_min.p, tr, o.states.p, elen, slen,
-                                               t.root_size, p.relative_radius_for_priors, o.prior.p, err.p); ::tsr::note_launch();
+    {
+        DBuf<double2> psum((size_t)nn * PK, st);
+        for (int d = (int)t.level_start.size() - 2; d >= 0; --d) {
+            uint32_t lo = t.level_start[d], hi = t.level_start[d + 1];
+            k_prior_sums<<<grid_for(hi - lo, BLK), BLK, 0, st>>>(lo, hi, t.level_order.p, t.children.p,
+                                                                t.node_to_leaf.p, o.states.p, elen, slen, psum.p); ::tsr::note_launch();
+        }
+        k_priors_h<<<grid_for(nl, 128), 128, 0, st>>>(nl, t.leaf_node.p, t.leaf_min.p, tr, o.states.p, elen, slen,
+                                                     psum.p, t.root_size, p.relative_radius_for_priors, o.prior.p,
+                                                     err.p); ::tsr::note_launch();
+    }
     o.stage_ms[3] = timer.lap();
     o.cone_count = read_scalar(cone_count.p, st);
     o.e_sum.alloc(nl, st); o.s_sum.alloc(nl, st); o.e_len.alloc(nl, st); o.s_len.alloc(nl, st); o.occ.alloc(nl, st);

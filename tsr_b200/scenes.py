@@ -205,8 +205,9 @@ def _jitter_normals(n, deg, rng):
 
 
 def render(prims, cams, width, height, f, noise_rel, jitter_deg, rng, stride=1,
-           target=None, conf_range=(1.0, 1.0), outlier_frac=0.0, name=""):
-    """Ray-cast every camera's depth map against the union of `prims`."""
+           target=None, conf_range=(1.0, 1.0), outlier_frac=0.0, name="", bound_radius=2.5):
+    """Ray-cast every camera's depth map against the union of `prims`, which
+    must lie inside the sphere of radius `bound_radius` around the origin."""
     cams = np.asarray(cams, float)
     ys, xs = np.mgrid[0:height:stride, 0:width:stride]
     px = (xs.ravel() + 0.5 - 0.5 * width) / f
@@ -217,6 +218,10 @@ def render(prims, cams, width, height, f, noise_rel, jitter_deg, rng, stride=1,
         d = fwd[None, :] + px[:, None] * right[None, :] + py[:, None] * down[None, :]
         zlen = np.linalg.norm(d, axis=1)
         d = d / zlen[:, None]
+        # only rays that meet the scene's bounding sphere can hit a primitive
+        b = d @ cam
+        near = b * b - (cam @ cam - bound_radius * bound_radius) >= 0
+        d, zlen = d[near], zlen[near]
         best = np.full(d.shape[0], np.inf)
         who = np.full(d.shape[0], -1)
         for pi, pr in enumerate(prims):
@@ -282,7 +287,7 @@ def _random_cams(rng, n, dmin, dmax):
     return v * rng.uniform(dmin, dmax, n)[:, None]
 
 
-def csg_scene(seed=0, n_target=4_000_000, width=1024, height=768, f=500.0, n_cams=120):
+def csg_scene(seed=0, n_target=4_000_000, width=1280, height=960, f=600.0, n_cams=120):
     """2 mm plate, cylinder r = 0.3, torus R = 0.5 / r = 0.1 in the box [-1, 1]^3."""
     rng = np.random.default_rng(seed)
     prims = [Box([-0.9, -0.9, -0.601], [0.9, 0.9, -0.599]),
