@@ -43,6 +43,9 @@ def make_scene(workload, seed):
     if workload == "csg4m":
         return scenes.csg_scene(seed=seed, n_target=4_000_000), \
             "csg: 2 mm plate + cylinder r=0.3 + torus R=0.5/r=0.1, 120 cameras at 1.5-12, 4M samples"
+    if workload == "csg1m":
+        return scenes.csg_scene(seed=seed, n_target=1_000_000), \
+            "csg (as csg4m) subsampled to 1M samples, for profiling"
     if workload == "sphere":
         return scenes.sphere_scene(seed=seed, stride=3), "unit sphere, 24 cameras, ~250k samples"
     if workload == "heldout16m":
@@ -122,6 +125,22 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def replica_throughput(samples_this_rank, seconds_this_rank, steps, dist=None):
+    """Whole-job samples/s of N independent replicas: every rank's samples
+    over the slowest rank's time (max over ranks)."""
+    if dist is None:
+        return samples_this_rank * steps / seconds_this_rank
+    import torch
+    t = torch.tensor([seconds_this_rank, float(samples_this_rank)], dtype=torch.float64)
+    if dist.get_backend() == "nccl":
+        t = t.cuda()
+    mx = t.clone()
+    dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+    tot = t.clone()
+    dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+    return float(tot[1]) * steps / float(mx[0])
+
+
 def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -192,10 +211,12 @@ def our_arm(args):
         oms = np.zeros(8, np.float32)
         core.lib.tsr_tree_stage_ms(tree, core._ptr(tms), 8)
         core.lib.tsr_occupancy_stage_ms(occ, core._ptr(oms), 8)
+        oc = core.tsr_occupancy_counts()
+        core._check(core.lib.tsr_occupancy_get_counts(occ, ctypes.byref(oc)))
         core.lib.tsr_mesh_free(mesh)
         core.lib.tsr_occupancy_free(occ)
         core.lib.tsr_tree_free(tree)
-        return tc, mc, tms, oms
+        return tc, mc, tms, oms, oc
 
     # ---- host buffers (pinned) for the e2e leg
     def pinned(a):
@@ -240,7 +261,7 @@ def our_arm(args):
     stage_sum = np.zeros(16)
     for i in range(args.steps):
         ev[i][0].record(stream)
-        tc, mc, tms, oms = device_step()
+        tc, mc, tms, oms, oc = device_step()
         ev[i][1].record(stream)
         stage_sum += np.concatenate([tms, oms])
     barrier()
@@ -250,22 +271,24 @@ def our_arm(args):
     t_value = max_over_ranks(t_value)
 
     # ---- timed: e2e through the public API from pinned host buffers
-    for _ in range(max(1, args.warmup // 2)):
-        e2e_step()
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        tree, mesh = e2e_step()
-    barrier()
-    t_e2e = max_over_ranks(time.perf_counter() - t0)
     h2d = n * (24 + 24 + 8 + 8 + 4 * scene.k) + scene.cams.nbytes
-    d2h = mesh.cases.nbytes + mesh.positions.nbytes + mesh.scales.nbytes + mesh.edge_keys.nbytes + \
-        mesh.triangles.nbytes
+    t_e2e, d2h = None, 0
+    if not args.value_only:
+        for _ in range(max(1, args.warmup // 2)):
+            e2e_step()
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            tree, mesh = e2e_step()
+        barrier()
+        t_e2e = max_over_ranks(time.perf_counter() - t0)
+        d2h = mesh.cases.nbytes + mesh.positions.nbytes + mesh.scales.nbytes + mesh.edge_keys.nbytes + \
+            mesh.triangles.nbytes
 
     # ---- roofline of the dominant kernel (per-launch algorithmic bytes / event time)
     stage_ms = stage_sum / args.steps
     names = ["tree.containment", "tree.sampling", "tree.balance", "tree.relayout", "tree.neighbors",
-             "tree.dual_cells", "", "", "occ.sampleness", "occ.flags", "occ.emptiness", "occ.priors", "occ.finalize",
+             "tree.dual_cells", "sub.sampling_eval", "sub.sampling_resolve", "occ.sampleness", "occ.flags", "occ.emptiness", "occ.priors", "occ.finalize",
              "", "", ""]
     stages = {nm: float(v) for nm, v in zip(names, stage_ms) if nm}
     K = scene.k
@@ -276,7 +299,7 @@ def our_arm(args):
     dom = max(alg, key=lambda k: stages[k])
     hbm, src = peaks()
     achieved = alg[dom] / (stages[dom] / 1e3) / 1e9
-    total_ms = sum(stages.values())
+    total_ms = sum(v for k, v in stages.items() if not k.startswith("sub."))
 
     world_samples = n * world
     line = {
@@ -288,9 +311,14 @@ def our_arm(args):
                    "mode": "plain FP32 field (compensated sums), FP64 topology",
                    "l2": "inputs %d MB > 126 MB L2; all buffers re-allocated each step" % (h2d // 2**20),
                    "parallelism": "replicas" if world > 1 else "single GPU",
-                   "nodes": Nn, "leaves": Nl, "dual_cells": tc.dual_cells, "triangles": mc.triangles},
-        "e2e": {"value": world_samples * args.steps / t_e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(d2h)},
+                   "nodes": Nn, "leaves": Nl, "dual_cells": tc.dual_cells, "triangles": mc.triangles,
+                   "accepted_pairs": {"sampleness": oc.accepted_sampleness, "emptiness": oc.accepted_emptiness},
+                   "nodes_visited": {"sampleness": oc.visited_sampleness, "emptiness": oc.visited_emptiness,
+                                     "priors": oc.visited_priors},
+                   "sampling": {"rounds": tc.sampling_rounds, "waves": tc.sampling_waves,
+                                "writers": tc.sampling_writers}},
+        "e2e": None if t_e2e is None else {"value": world_samples * args.steps / t_e2e, "unit": UNIT,
+                                            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(launches),
         "stage_ms": {k: round(v, 3) for k, v in stages.items()},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm,
@@ -319,8 +347,9 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="csg4m", choices=["csg4m", "sphere", "heldout16m"])
+    ap.add_argument("--workload", default="csg4m", choices=["csg4m", "csg1m", "sphere", "heldout16m"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--value-only", action="store_true", help="skip the e2e leg (profiling runs)")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)

@@ -89,11 +89,22 @@ typedef struct {
     uint32_t max_depth;
     uint32_t sampling_rounds;          /* rounds of the order-exact sampling schedule */
     uint64_t sampling_writers;         /* sample sides that had to create nodes */
+    uint32_t sampling_waves;           /* conflict-resolution waves over all rounds */
+    uint32_t reserved;
 } tsr_tree_counts;
 
 typedef struct {
     uint64_t vertices, triangles, active_cells;
 } tsr_mesh_counts;
+
+typedef struct {
+    uint64_t links;                    /* camera-to-sample links (N * K) */
+    uint64_t accepted_sampleness;      /* (link, leaf) pairs addKernel accepted, SAMPLENESS pass */
+    uint64_t accepted_emptiness;       /* ... EMPTINESS pass */
+    uint64_t visited_sampleness;       /* tree nodes tested against a cone, SAMPLENESS pass */
+    uint64_t visited_emptiness;        /* ... EMPTINESS pass */
+    uint64_t visited_priors;           /* tree nodes classified by the prior sphere queries */
+} tsr_occupancy_counts;
 
 typedef struct tsr_tree tsr_tree;
 typedef struct tsr_occupancy tsr_occupancy;
@@ -146,6 +157,9 @@ TSR_API tsr_status tsr_occupancy_compute(const tsr_tree *tree, const tsr_cameras
                                  const tsr_params *params, int mode, void *cuda_stream,
                                  tsr_occupancy **out_occupancy);
 TSR_API void tsr_occupancy_free(tsr_occupancy *occ);
+/* Work counters of the last field computation (no counterpart in the
+ * reference; instrumentation). */
+TSR_API tsr_status tsr_occupancy_get_counts(const tsr_occupancy *occ, tsr_occupancy_counts *out);
 TSR_API tsr_status tsr_occupancy_copy(const tsr_occupancy *occ, tsr_field field, void *host_dst);
 
 TSR_API tsr_status tsr_dmc_extract(const tsr_tree *tree, const tsr_occupancy *occ, void *cuda_stream,

@@ -49,11 +49,17 @@ class tsr_cameras_view(ctypes.Structure):
 
 class tsr_tree_counts(ctypes.Structure):
     _fields_ = [("nodes", _U64), ("leaves", _U64), ("dual_cells", _U64), ("neighbor_entries", _U64),
-                ("max_depth", _U32), ("sampling_rounds", _U32), ("sampling_writers", _U64)]
+                ("max_depth", _U32), ("sampling_rounds", _U32), ("sampling_writers", _U64),
+                ("sampling_waves", _U32), ("reserved", _U32)]
 
 
 class tsr_mesh_counts(ctypes.Structure):
     _fields_ = [("vertices", _U64), ("triangles", _U64), ("active_cells", _U64)]
+
+
+class tsr_occupancy_counts(ctypes.Structure):
+    _fields_ = [("links", _U64), ("accepted_sampleness", _U64), ("accepted_emptiness", _U64),
+                ("visited_sampleness", _U64), ("visited_emptiness", _U64), ("visited_priors", _U64)]
 
 
 lib = ctypes.CDLL(str(_LIB_PATH))
@@ -75,6 +81,7 @@ _sig = {
     "tsr_tree_stage_ms": (ctypes.c_int, [_P, _P, ctypes.c_int]),
     "tsr_occupancy_compute": (ctypes.c_int, [_P, _P, _P, ctypes.c_int, _P, _P]),
     "tsr_occupancy_free": (None, [_P]),
+    "tsr_occupancy_get_counts": (ctypes.c_int, [_P, _P]),
     "tsr_occupancy_copy": (ctypes.c_int, [_P, ctypes.c_int, _P]),
     "tsr_occupancy_stage_ms": (ctypes.c_int, [_P, _P, ctypes.c_int]),
     "tsr_dmc_extract": (ctypes.c_int, [_P, _P, _P, _P]),

@@ -150,6 +150,8 @@ tsr_status tsr_tree_get_counts(const tsr_tree *t, tsr_tree_counts *out) {
         out->max_depth = t->max_depth;
         out->sampling_rounds = t->sampling_rounds;
         out->sampling_writers = t->sampling_writers;
+        out->sampling_waves = t->sampling_waves;
+        out->reserved = 0;
     });
 }
 
@@ -268,6 +270,18 @@ tsr_status tsr_occupancy_compute(const tsr_tree *tree, const tsr_cameras_view *c
 }
 
 void tsr_occupancy_free(tsr_occupancy *o) { delete o; }
+
+tsr_status tsr_occupancy_get_counts(const tsr_occupancy *o, tsr_occupancy_counts *out) {
+    return guarded([&] {
+        if (!o || !out) fail(TSR_ERR_INVALID_ARG, "null argument");
+        out->links = o->links;
+        out->accepted_sampleness = o->accepted[1];
+        out->accepted_emptiness = o->accepted[0];
+        out->visited_sampleness = o->visits[1];
+        out->visited_emptiness = o->visits[0];
+        out->visited_priors = o->visits[2];
+    });
+}
 
 tsr_status tsr_occupancy_copy(const tsr_occupancy *o, tsr_field field, void *dst) {
     return guarded([&] {

@@ -13,7 +13,7 @@ struct tsr_tree {
     double root_size = 0;
     uint32_t n_nodes = 0, n_leaves = 0, max_depth = 0, n_cells = 0;
     uint64_t n_nb = 0;
-    uint32_t sampling_rounds = 0;
+    uint32_t sampling_rounds = 0, sampling_waves = 0;
     uint64_t sampling_writers = 0;
 
     // final node arrays (reference order after Nodes::reorder)
@@ -42,7 +42,9 @@ struct tsr_occupancy {
     tsr::DBuf<uint32_t> states;
     double cone_count = 0;
     float stage_ms[8] = {0};
-    uint64_t accepted[2] = {0, 0};
+    uint64_t accepted[2] = {0, 0};   // [EMPTINESS, SAMPLENESS]
+    uint64_t visits[3] = {0, 0, 0};  // nodes tested: EMPTINESS, SAMPLENESS, priors
+    uint64_t links = 0;
 };
 
 struct tsr_mesh {

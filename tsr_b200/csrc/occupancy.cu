@@ -263,6 +263,229 @@ __global__ void __launch_bounds__(128) k_cone_pass(uint64_t nlinks, LinkIn in, T
     }
 }
 
+// ---------------------------------------------- persistent cone traversal
+// Thread-per-link depth-first traversal (the per-link LeavesIterator with a
+// ConeNodesChecker) run by persistent threads: a lane whose traversal ends
+// immediately takes the next link, fetched per warp in one atomic batch, so
+// lanes do not idle behind the warp's longest link.  Child boxes are derived
+// from the parent's box in the link's FP32 frame (no node-geometry loads
+// inside the loop); node records read per visit are the child block index and,
+// for EMPTINESS, the state word.
+
+// Conservative box test with an absolute slack for the FP32 box recurrence.
+__device__ inline bool cone_box_separated_pt(const ConeF &c, F3 bmin, float size) {
+    float h = 0.5f * size;
+    F3 ctr = bmin + f3(h, h, h);
+    float mag = fabsf(ctr.x) + fabsf(ctr.y) + fabsf(ctr.z);
+    float hs = h + 2e-6f * mag;
+    F3 u = ctr - c.end;
+    float te = fdot(u, c.m) * c.inv_denom;
+    float dt = hs * c.n1 * fabsf(c.inv_denom);
+    float slack = 1e-4f * (dt + fabsf(te)) + 1e-6f;
+    if (te + dt < c.t_start_e - slack) return true;
+    if (te - dt >= slack) return true;
+    if (1.0f + te + dt <= 0.0f) return true;
+    F3 q = u - c.axis * te;
+    float qn = sqrtf(fdot(q, q));
+    float tmax = fminf(1.0f + te + dt, 1.0f);
+    float bound = qn - hs * 1.7320508f - dt * c.full;
+    return bound > tmax * c.radius * 1.0001f + 1e-4f * (qn + hs + dt * c.full);
+}
+
+constexpr int PT_BLOCK = 128;
+
+template <int TYPE>
+__global__ void __launch_bounds__(PT_BLOCK) k_cone_pt(uint64_t nlinks, const uint32_t *order, LinkIn in, TreeIn tr,
+                                                      uint32_t *states, float2 *ksum, float2 *clen,
+                                                      double *cone_count, unsigned long long *accepted,
+                                                      unsigned long long *next_link, unsigned long long *visits,
+                                                      int *err) {
+    const unsigned FULL = 0xffffffffu;
+    const unsigned lane = threadIdx.x & 31;
+    const uint32_t req = (TYPE == EMPTINESS) ? FLAG_SAMPLENESS : 0u;
+    const uint32_t leaf_flag = (TYPE == EMPTINESS) ? FLAG_EMPTINESS : FLAG_SAMPLENESS;
+    const float root_size_f = (float)in.root_size;
+    uint32_t st_node[MAX_TREE_DEPTH];
+    uint8_t st_next[MAX_TREE_DEPTH];
+    F3 st_min[MAX_TREE_DEPTH];
+    int sp = 0;
+    uint32_t top_node = 0, top_c0 = 0, top_next = 0;
+    F3 top_min = f3(0.f, 0.f, 0.f);
+    uint32_t base = 0, max_depth = 0;
+    ConeF c;
+    float wlen = 0.f, fconf = 0.f;
+    bool done = false;
+    double count = 0.0;
+    unsigned long long acc = 0, nvis = 0;
+
+    auto visit_leaf = [&](uint32_t node, F3 bmin, float size) {
+        float h = 0.5f * size;
+        float val;
+        if (!eval_kernel(c, bmin + f3(h, h, h), TYPE == SAMPLENESS, fconf, &val)) return;
+        uint32_t leaf = tr.node_to_leaf[node];
+        add_comp(&ksum[leaf], val);
+        add_comp(&clen[leaf], wlen);
+        if ((states[node] & leaf_flag) == 0) atomicOr(&states[node], leaf_flag);
+        ++acc;
+    };
+
+    while (true) {
+        bool need = (sp == 0) && !done;
+        unsigned nm = __ballot_sync(FULL, need);
+        if (nm) {
+            int leader = __ffs(nm) - 1;
+            unsigned long long b = 0;
+            if ((int)lane == leader) b = atomicAdd(next_link, (unsigned long long)__popc(nm));
+            b = __shfl_sync(FULL, b, leader);
+            if (need) {
+                uint64_t i = b + __popc(nm & ((1u << lane) - 1u));
+                if (i >= nlinks) {
+                    done = true;
+                } else do {
+                    // ---- set-up of link l (Occupancy.cpp:174-201), FP64
+                    uint64_t l = order ? order[i] : i;
+                    uint32_t s = (uint32_t)(l / in.k);
+                    uint32_t cam = in.links[l];
+                    if (cam == INVALID || cam >= in.ncams) break;
+                    D3 p = in.pos[s];
+                    D3 n = in.nrm[s];
+                    D3 cwp = in.cams[cam];
+                    double kernel_r = in.h_o * in.scale[s];
+                    D3 apex_d{cwp.x - p.x, cwp.y - p.y, cwp.z - p.z};
+                    D3 end_d{0.0, 0.0, 0.0};
+                    double cone_len = REAL_MAX;
+                    if (TYPE == SAMPLENESS) {
+                        D3 cs{-apex_d.x, -apex_d.y, -apex_d.z};
+                        double total = sqrt(cs.x * cs.x + cs.y * cs.y + cs.z * cs.z);
+                        cone_len = kernel_r * in.rel_cone;
+                        double hh = cone_len * 0.5;
+                        end_d = D3{cs.x / total * hh, cs.y / total * hh, cs.z / total * hh};
+                    }
+                    D3 m{-n.x, -n.y, -n.z};
+                    D3 axis{end_d.x - apex_d.x, end_d.y - apex_d.y, end_d.z - apex_d.z};
+                    double full = sqrt(axis.x * axis.x + axis.y * axis.y + axis.z * axis.z);
+                    double length = cone_len < full ? cone_len : full;
+                    double denom = axis.x * m.x + axis.y * m.y + axis.z * m.z;
+                    if (!(full > EPS) || !(kernel_r > 0.0) || fabs(denom) <= EPS * full) break;   // isDegenerated
+                    double conf = in.conf[s];
+                    if (TYPE == EMPTINESS) count += conf;
+                    wlen = (float)(conf * length);
+                    fconf = (float)conf;
+                    max_depth = (uint32_t)ceil(log2(in.root_size / (in.scale[s] * in.h_svo))) + MAX_DEPTH_DIFFERENCE;
+                    c.apex = f3((float)apex_d.x, (float)apex_d.y, (float)apex_d.z);
+                    c.end = f3((float)end_d.x, (float)end_d.y, (float)end_d.z);
+                    c.axis = f3((float)axis.x, (float)axis.y, (float)axis.z);
+                    c.m = f3((float)m.x, (float)m.y, (float)m.z);
+                    c.radius = (float)kernel_r;
+                    c.full = (float)full;
+                    c.length = (float)length;
+                    c.inv_denom = (float)(1.0 / denom);
+                    c.a_over_l = (float)(full / length);
+                    c.t_start_e = (float)(-length / full);
+                    c.n1 = fabsf(c.m.x) + fabsf(c.m.y) + fabsf(c.m.z);
+                    // start at the deepest node containing the cut cone's bounding box
+                    F3 p0 = c.end + c.axis * c.t_start_e;
+                    F3 lo = f3(fminf(p0.x, c.end.x) - c.radius, fminf(p0.y, c.end.y) - c.radius, fminf(p0.z, c.end.z) - c.radius);
+                    F3 hi = f3(fmaxf(p0.x, c.end.x) + c.radius, fmaxf(p0.y, c.end.y) + c.radius, fmaxf(p0.z, c.end.z) + c.radius);
+                    uint32_t start = 0;
+                    base = 0;
+                    F3 smin = rel(tr.nmin[0], p);
+                    float ssize = root_size_f;
+                    while (tr.children[start] != INVALID && base + 1 <= max_depth) {
+                        float cs = 0.5f * ssize;
+                        float margin = 1e-5f * ssize;
+                        F3 ctr = smin + f3(cs, cs, cs);
+                        const float l3[3] = {lo.x, lo.y, lo.z}, h3[3] = {hi.x, hi.y, hi.z}, c3[3] = {ctr.x, ctr.y, ctr.z};
+                        uint32_t digit = 0;
+                        bool inside = true;
+                        for (int a = 0; a < 3; ++a) {
+                            if (h3[a] < c3[a] - margin) continue;
+                            if (l3[a] > c3[a] + margin) { digit |= 1u << a; continue; }
+                            inside = false;
+                        }
+                        if (!inside) break;
+                        start = tr.children[start] + digit;
+                        smin = rel(tr.nmin[start], p);
+                        ssize = cs;
+                        ++base;
+                    }
+                    if (req && (states[start] & req) != req) break;
+                    if (cone_box_separated_pt(c, smin, ssize)) break;
+                    if (tr.children[start] == INVALID) { visit_leaf(start, smin, ssize); break; }
+                    if (base + 1 > max_depth) break;
+                    top_node = start;
+                    top_c0 = tr.children[start];
+                    top_next = 0;
+                    top_min = smin;
+                    sp = 1;
+                } while (0);
+            }
+        }
+        if (__all_sync(FULL, done && sp == 0)) break;
+        if (sp > 0) {
+            // one step of the depth-first traversal (NodesIterator.cpp:38-86);
+            // the top of the stack lives in registers, the rest in local memory
+            if (top_next == 8) {
+                --sp;
+                if (sp > 0) {
+                    top_node = st_node[sp - 1];
+                    top_next = st_next[sp - 1];
+                    top_min = st_min[sp - 1];
+                    top_c0 = tr.children[top_node];
+                }
+            } else {
+                uint32_t ci = top_next++;
+                uint32_t idx = top_c0 + ci;
+                ++nvis;
+                uint32_t d = base + (uint32_t)sp;
+                float size = ldexpf(root_size_f, -(int)d);
+                F3 bmin = f3((ci & 1u) ? top_min.x + size : top_min.x, (ci & 2u) ? top_min.y + size : top_min.y,
+                             (ci & 4u) ? top_min.z + size : top_min.z);
+                if (!(req && (states[idx] & req) != req)) {
+                    uint32_t cc0 = tr.children[idx];
+                    if (cc0 == INVALID) {
+                        // a leaf: addKernel's exact test decides, no box test needed
+                        visit_leaf(idx, bmin, size);
+                    } else if (d + 1 <= max_depth && !cone_box_separated_pt(c, bmin, size)) {
+                        if (sp >= MAX_TREE_DEPTH) {
+                            atomicExch(err, 1);
+                        } else {
+                            st_node[sp - 1] = top_node;
+                            st_next[sp - 1] = (uint8_t)top_next;
+                            st_min[sp - 1] = top_min;
+                            top_node = idx;
+                            top_c0 = cc0;
+                            top_next = 0;
+                            top_min = bmin;
+                            ++sp;
+                        }
+                    }
+                }
+            }
+        }
+    }
+    // warp-level totals (no block barrier: warps finish independently)
+    for (int o = 16; o; o >>= 1) {
+        count += __shfl_xor_sync(FULL, count, o);
+        acc += __shfl_xor_sync(FULL, acc, o);
+        nvis += __shfl_xor_sync(FULL, nvis, o);
+    }
+    if (lane == 0) {
+        if (TYPE == EMPTINESS && count != 0.0) atomicAdd(cone_count, count);
+        if (acc) atomicAdd(accepted, acc);
+        if (nvis) atomicAdd(visits, nvis);
+    }
+}
+
+__global__ void k_link_cameras(uint64_t nlinks, const uint32_t *links, uint32_t ncams, uint32_t *keys,
+                               uint32_t *vals) {
+    uint64_t l = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= nlinks) return;
+    uint32_t c = links[l];
+    keys[l] = (c == INVALID || c >= ncams) ? ncams : c;
+    vals[l] = (uint32_t)l;
+}
+
 // forwardAnyChildStateFlag, one level bottom-up.
 __global__ void k_forward_flag(uint32_t lo, uint32_t hi, const uint32_t *order, const uint32_t *children,
                                uint32_t *states, uint32_t flag) {
@@ -323,19 +546,42 @@ __device__ inline bool box_inside_sphere(const D3 &mn, double sz, const D3 &c, d
     return dx * dx + dy * dy + dz * dz <= r * r * (1.0 - 1e-9);
 }
 
+// Node record for the prior queries: geometry, child block and the
+// SAMPLENESS flag in one aligned 32-byte sector, so a visit is one load.
+struct __align__(32) PNode {
+    double x, y, z;
+    uint32_t children;
+    uint32_t flagged;
+};
+
+__global__ void k_pack_nodes(uint32_t nn, const uint32_t *children, const D3 *nmin, const uint32_t *states,
+                             PNode *out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nn) return;
+    D3 m = nmin[i];
+    PNode r;
+    r.x = m.x;
+    r.y = m.y;
+    r.z = m.z;
+    r.children = children[i];
+    r.flagged = states[i] & FLAG_SAMPLENESS;
+    out[i] = r;
+}
+
 // Occupancy::computePriors (Occupancy.cpp:530-568) with a
 // SphereNodeStatesChecker (SphereNodeStatesChecker.cpp:28-36).  The set of
 // summed leaves is the reference's: SAMPLENESS-flagged leaves at most three
 // levels below the query leaf whose box meets the sphere (the exact FP64
-// test); subtrees wholly inside the sphere are added from psum.
+// test); subtrees wholly inside the sphere are added from psum, whose row 0
+// of a leaf is the leaf's own (emptiness, sampleness) cone-length pair.
 __global__ void __launch_bounds__(128) k_priors_h(uint32_t nl, const uint32_t *leaf_node, const D3 *leaf_min,
-                                                  TreeIn tr, const uint32_t *states, const float2 *elen,
-                                                  const float2 *slen, const double2 *psum, double root_size,
-                                                  double rel_radius, double *prior, int *err) {
+                                                  const uint8_t *depth, const PNode *pn, const double2 *psum,
+                                                  double root_size, double rel_radius, double *prior,
+                                                  unsigned long long *visits, int *err) {
     uint32_t l = blockIdx.x * blockDim.x + threadIdx.x;
     if (l >= nl) return;
     uint32_t node = leaf_node[l];
-    uint32_t ld = tr.depth[node];
+    uint32_t ld = depth[node];
     double size = size_at(root_size, ld);
     D3 mn = leaf_min[l];
     double half = dmul(0.5, size);
@@ -343,57 +589,61 @@ __global__ void __launch_bounds__(128) k_priors_h(uint32_t nl, const uint32_t *l
     double radius = dmul(size, rel_radius);
     uint32_t max_depth = ld + MAX_DEPTH_DIFFERENCE;
     double eL = 0.0, sL = 0.0;
+    unsigned long long nvis = 0;
     // returns 0 = ignored, 1 = add subtree sum, 2 = visit / descend
-    auto classify = [&](uint32_t n, const D3 &bmn, double sz, uint32_t depth) -> int {
-        if ((states[n] & FLAG_SAMPLENESS) == 0) return 0;
-        if (depth > max_depth) return 0;
+    auto classify = [&](const PNode &r, double sz, uint32_t d) -> int {
+        if (!r.flagged) return 0;
+        if (d > max_depth) return 0;
+        D3 bmn{r.x, r.y, r.z};
         D3 bmx{dadd(bmn.x, sz), dadd(bmn.y, sz), dadd(bmn.z, sz)};
         if (!aabb_sphere(bmn, bmx, center, radius)) return 0;
-        if (max_depth - depth < (uint32_t)PK && box_inside_sphere(bmn, sz, center, radius)) return 1;
+        if (max_depth - d < (uint32_t)PK && box_inside_sphere(bmn, sz, center, radius)) return 1;
         return 2;
     };
-    auto add_sum = [&](uint32_t n, uint32_t depth) {
-        double2 v = psum[(size_t)n * PK + (max_depth - depth)];
+    auto add_row = [&](uint32_t n, uint32_t k) {
+        double2 v = psum[(size_t)n * PK + k];
         eL += v.x;
         sL += v.y;
     };
-    auto visit = [&](uint32_t n) {
-        uint32_t leaf = tr.node_to_leaf[n];
-        eL += comp_value(elen[leaf]);
-        sL += comp_value(slen[leaf]);
-    };
-    int rc = classify(0, tr.nmin[0], root_size, 0);
+    PNode r0 = pn[0];
+    int rc = classify(r0, root_size, 0);
     if (rc == 1) {
-        add_sum(0, 0);
+        add_row(0, max_depth);
     } else if (rc == 2) {
-        if (tr.children[0] == INVALID) {
-            visit(0);
+        if (r0.children == INVALID) {
+            add_row(0, 0);
         } else {
-            uint32_t st_node[MAX_TREE_DEPTH];
+            uint32_t st_c0[MAX_TREE_DEPTH];
             uint8_t st_next[MAX_TREE_DEPTH];
             int sp = 1;
-            st_node[0] = 0;
-            st_next[0] = 0;
+            uint32_t top_c0 = r0.children, top_next = 0;
             while (sp > 0) {
-                int t = sp - 1;
-                if (st_next[t] == 8) { --sp; continue; }
-                uint32_t ci = st_next[t]++;
-                uint32_t idx = tr.children[st_node[t]] + ci;
-                uint32_t d = (uint32_t)t + 1;
+                if (top_next == 8) {
+                    --sp;
+                    if (sp > 0) { top_c0 = st_c0[sp - 1]; top_next = st_next[sp - 1]; }
+                    continue;
+                }
+                uint32_t idx = top_c0 + top_next++;
+                uint32_t d = (uint32_t)sp;
                 double sz = size_at(root_size, d);
-                int c = classify(idx, tr.nmin[idx], sz, d);
+                ++nvis;
+                PNode r = pn[idx];
+                int c = classify(r, sz, d);
                 if (c == 0) continue;
-                if (c == 1) { add_sum(idx, d); continue; }
-                if (tr.children[idx] == INVALID) { visit(idx); continue; }
+                if (c == 1) { add_row(idx, max_depth - d); continue; }
+                if (r.children == INVALID) { add_row(idx, 0); continue; }
                 if (d + 1 > max_depth) continue;
                 if (sp >= MAX_TREE_DEPTH) { atomicExch(err, 2); break; }
-                st_node[sp] = idx;
-                st_next[sp] = 0;
+                st_c0[sp - 1] = top_c0;
+                st_next[sp - 1] = (uint8_t)top_next;
+                top_c0 = r.children;
+                top_next = 0;
                 ++sp;
             }
         }
     }
     prior[l] = eL / (eL + sL);
+    if (nvis) atomicAdd(visits, nvis);
 }
 
 // Occupancy::getOccupancy (Occupancy.cpp:570-587), FP64.
@@ -457,7 +707,7 @@ void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_
     o.states.zero();
     DBuf<double> cone_count(1, st);
     cone_count.zero();
-    DBuf<unsigned long long> accepted(2, st);
+    DBuf<unsigned long long> accepted(5, st);   // accepted E, S; visits E, S; prior visits
     accepted.zero();
     DBuf<int> err(1, st);
     err.zero();
@@ -466,11 +716,46 @@ void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_
               p.max_relative_sampling_distance, p.bandwidth_factor, p.relative_sample_cone_length, t.root_size};
     TreeIn tr{t.children.p, t.depth.p, t.nmin.p, t.node_to_leaf.p};
     uint64_t nlinks = (uint64_t)t.n_samples * t.k;
+    o.links = nlinks;
     unsigned grid = (unsigned)((nlinks + 127) / 128);
     if (grid == 0) grid = 1;
-    k_cone_pass<SAMPLENESS><<<grid, 128, 0, st>>>(nlinks, in, tr, o.states.p, ssum, slen, cone_count.p, accepted.p + 1,
-                                                  err.p); ::tsr::note_launch();
+    DBuf<unsigned long long> next_link(1, st);
+    unsigned pt_grid = 0;
+    {
+        int dev = 0, sms = 0, per_sm = 0;
+        TSR_CUDA(cudaGetDevice(&dev));
+        TSR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        TSR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cone_pt<EMPTINESS>, PT_BLOCK, 0));
+        pt_grid = (unsigned)(sms * (per_sm > 0 ? per_sm : 1));
+    }
+    // TSR_CONE_KERNEL=thread selects the one-thread-per-link kernel (same
+    // traversal and results, no persistent scheduling) for comparisons
+    const char *kenv = getenv("TSR_CONE_KERNEL");
+    const bool per_thread = kenv && kenv[0] == 't';
+    if (per_thread) {
+        k_cone_pass<SAMPLENESS><<<grid, 128, 0, st>>>(nlinks, in, tr, o.states.p, ssum, slen, cone_count.p,
+                                                      accepted.p + 1, err.p);
+    } else {
+        next_link.zero();
+        k_cone_pt<SAMPLENESS><<<pt_grid, PT_BLOCK, 0, st>>>(nlinks, nullptr, in, tr, o.states.p, ssum, slen,
+                                                           cone_count.p, accepted.p + 1, next_link.p,
+                                                           accepted.p + 3, err.p);
+    }
+    ::tsr::note_launch();
     o.stage_ms[0] = timer.lap();
+    // EMPTINESS links grouped by camera (stable, so sample order is kept
+    // within a camera): a warp's cones then share their apex
+    DBuf<uint32_t> order((size_t)nlinks, st);
+    {
+        DBuf<uint32_t> ckeys((size_t)nlinks, st), ckeys2((size_t)nlinks, st), vals((size_t)nlinks, st);
+        k_link_cameras<<<grid_for(nlinks, BLK), BLK, 0, st>>>(nlinks, t.links.p, cv.count, ckeys.p, vals.p); ::tsr::note_launch();
+        int bits = 1;
+        while ((1u << bits) <= cv.count) ++bits;
+        size_t tmp = 0;
+        TSR_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, ckeys.p, ckeys2.p, vals.p, order.p, (int)nlinks, 0, bits, st));
+        DBuf<uint8_t> tb(tmp, st);
+        TSR_CUDA(cub::DeviceRadixSort::SortPairs(tb.p, tmp, ckeys.p, ckeys2.p, vals.p, order.p, (int)nlinks, 0, bits, st));
+    }
     // forwardAnyChildStateFlag(0, SAMPLENESS) before the EMPTINESS pass (Occupancy.cpp:141-142)
     for (int d = (int)t.level_start.size() - 2; d >= 0; --d) {
         uint32_t lo = t.level_start[d], hi = t.level_start[d + 1];
@@ -478,8 +763,16 @@ void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_
                                                               FLAG_SAMPLENESS); ::tsr::note_launch();
     }
     o.stage_ms[1] = timer.lap();
-    k_cone_pass<EMPTINESS><<<grid, 128, 0, st>>>(nlinks, in, tr, o.states.p, esum, elen, cone_count.p, accepted.p,
-                                                 err.p); ::tsr::note_launch();
+    if (per_thread) {
+        k_cone_pass<EMPTINESS><<<grid, 128, 0, st>>>(nlinks, in, tr, o.states.p, esum, elen, cone_count.p, accepted.p,
+                                                     err.p);
+    } else {
+        next_link.zero();
+        k_cone_pt<EMPTINESS><<<pt_grid, PT_BLOCK, 0, st>>>(nlinks, order.p, in, tr, o.states.p, esum, elen,
+                                                          cone_count.p, accepted.p, next_link.p, accepted.p + 2,
+                                                          err.p);
+    }
+    ::tsr::note_launch();
     o.stage_ms[2] = timer.lap();
     o.prior.alloc(nl, st);
     {
@@ -489,9 +782,12 @@ void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_
             k_prior_sums<<<grid_for(hi - lo, BLK), BLK, 0, st>>>(lo, hi, t.level_order.p, t.children.p,
                                                                 t.node_to_leaf.p, o.states.p, elen, slen, psum.p); ::tsr::note_launch();
         }
-        k_priors_h<<<grid_for(nl, 128), 128, 0, st>>>(nl, t.leaf_node.p, t.leaf_min.p, tr, o.states.p, elen, slen,
-                                                     psum.p, t.root_size, p.relative_radius_for_priors, o.prior.p,
-                                                     err.p); ::tsr::note_launch();
+        DBuf<PNode> pn(nn, st);
+        k_pack_nodes<<<grid_for(nn, BLK), BLK, 0, st>>>(nn, t.children.p, t.nmin.p, o.states.p, pn.p); ::tsr::note_launch();
+        k_priors_h<<<grid_for(nl, 128), 128, 0, st>>>(nl, t.leaf_node.p, t.leaf_min.p, t.depth.p, pn.p, psum.p,
+                                                     t.root_size, p.relative_radius_for_priors, o.prior.p,
+                                                     accepted.p + 4, err.p);
+        ::tsr::note_launch();
     }
     o.stage_ms[3] = timer.lap();
     o.cone_count = read_scalar(cone_count.p, st);
@@ -500,11 +796,14 @@ void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_
                                                  p.confidence_threshold, o.e_sum.p, o.s_sum.p, o.e_len.p, o.s_len.p,
                                                  o.occ.p); ::tsr::note_launch();
     o.stage_ms[4] = timer.lap();
-    unsigned long long a[2];
-    TSR_CUDA(cudaMemcpyAsync(a, accepted.p, 16, cudaMemcpyDeviceToHost, st));
+    unsigned long long a[5];
+    TSR_CUDA(cudaMemcpyAsync(a, accepted.p, sizeof(a), cudaMemcpyDeviceToHost, st));
     int e = read_scalar(err.p, st);
     o.accepted[0] = a[0];
     o.accepted[1] = a[1];
+    o.visits[0] = a[2];
+    o.visits[1] = a[3];
+    o.visits[2] = a[4];
     if (e) fail(TSR_ERR_DEVICE_ASSERT, "occupancy traversal exceeded its stack bound");
     TSR_CUDA(cudaGetLastError());
 }

@@ -299,39 +299,85 @@ __global__ void k_sampling_eval(uint32_t m, const uint32_t *keys, NV v, Root roo
     if (e) atomicExch(err, e);
 }
 
-// Writers and unresolved sides claim their descent leaf with their key.
-__global__ void k_sampling_mark(uint32_t m, const uint32_t *keys, const uint8_t *status, const uint8_t *unres,
-                                const uint32_t *dleaf, uint32_t *mark) {
+// Conflict resolution of a round as a breadth-first search in key order.
+// A side is unresolved when a leaf it depends on (its witness if reliable;
+// every leaf its search read and its descent leaf if it is a writer) is
+// claimed by an earlier writer or unresolved side; claims propagate wave by
+// wave from the writers.  The result is the least fixed point, i.e. exactly
+// what a sequential pass in key order computes.
+
+// Wave members claim their descent leaf; leaves whose claim dropped are
+// recorded for the witness scan.
+__global__ void k_wave_mark(uint32_t nf, const uint32_t *frontier, const uint32_t *keys, const uint32_t *dleaf,
+                            uint32_t *mark, uint32_t *touched, uint32_t *ntouched) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= m) return;
-    if (status[i] == 2 || unres[i]) atomicMin(&mark[dleaf[i]], keys[i]);
+    if (i >= nf) return;
+    uint32_t p = frontier[i];
+    uint32_t x = dleaf[p], k = keys[p];
+    uint32_t old = atomicMin(&mark[x], k);
+    if (old > k) touched[atomicAdd(ntouched, 1u)] = x;
 }
 
-// A side is unresolved when a leaf it depends on is claimed by an earlier
-// writer or unresolved side.
-__global__ void k_sampling_conflict(uint32_t m, const uint32_t *keys, NV v, Root root, const D3 *pos,
-                                    const D3 *nrm, const double *scale, double h_svo, const uint8_t *status,
-                                    const uint32_t *witness, const uint32_t *dleaf, const uint32_t *mark,
-                                    uint8_t *unres, uint32_t *changed, int *err) {
+// Reliable sides witnessed by a leaf claimed by an earlier key become
+// unresolved (one warp per touched leaf).
+__global__ void k_wave_witness(uint32_t nt, const uint32_t *touched, const uint32_t *seg_lo, const uint32_t *seg_hi,
+                               const uint32_t *by_witness, const uint32_t *keys, const uint32_t *mark,
+                               uint32_t *unres, uint32_t *next, uint32_t *nnext) {
+    uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (w >= nt) return;
+    uint32_t x = touched[w];
+    uint32_t lo = seg_lo[x];
+    if (lo == INVALID) return;
+    uint32_t hi = seg_hi[x], mk = mark[x];
+    for (uint32_t j = lo + lane; j < hi; j += 32) {
+        uint32_t q = by_witness[j];
+        if (keys[q] > mk && atomicExch(&unres[q], 1u) == 0u) next[atomicAdd(nnext, 1u)] = q;
+    }
+}
+
+// Dependency lists: the leaves each pending side depends on (its witness if
+// reliable; the leaves its search read plus its descent leaf if a writer).
+// Phase 0 counts, phase 1 writes (leaf, side) pairs at `off`.
+__global__ void k_sens(uint32_t m, const uint32_t *keys, NV v, Root root, const D3 *pos, const D3 *nrm,
+                       const double *scale, double h_svo, const uint8_t *status, const uint32_t *witness,
+                       const uint32_t *dleaf, uint32_t *cnt, const uint32_t *off, uint32_t *skeys, uint32_t *svals,
+                       int phase, int *err) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= m || unres[i]) return;
-    uint32_t key = keys[i];
-    bool conflict = false;
+    if (i >= m) return;
     if (status[i] == 1) {
-        conflict = mark[witness[i]] < key;
-    } else {
-        conflict = mark[dleaf[i]] < key;
-        if (!conflict) {
-            SampleRef q = sample_side(key, pos, nrm, scale, h_svo);
-            int e = 0;
-            find_reliable_v(v, root, key, q, [&](uint32_t leaf) { if (mark[leaf] < key) conflict = true; }, &e);
-            if (e) atomicExch(err, e);
-        }
+        if (phase == 0) cnt[i] = 1;
+        else { skeys[off[i]] = witness[i]; svals[off[i]] = i; }
+        return;
     }
-    if (conflict) {
-        unres[i] = 1;
-        *changed = 1;
-    }
+    uint32_t key = keys[i];
+    SampleRef q = sample_side(key, pos, nrm, scale, h_svo);
+    int e = 0;
+    uint32_t c = 0, o = phase ? off[i] : 0;
+    find_reliable_v(v, root, key, q, [&](uint32_t leaf) {
+        if (phase) { skeys[o + c] = leaf; svals[o + c] = i; }
+        ++c;
+    }, &e);
+    if (phase) { skeys[o + c] = dleaf[i]; svals[o + c] = i; }
+    else cnt[i] = c + 1;
+    if (e) atomicExch(err, e);
+}
+
+__global__ void k_writer_list(uint32_t m, const uint8_t *status, uint32_t *writers, uint32_t *nwri) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m && status[i] == 2) writers[atomicAdd(nwri, 1u)] = i;
+}
+
+__global__ void k_segments(uint32_t n, const uint32_t *sorted, uint32_t *seg_lo, uint32_t *seg_hi) {
+    uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    uint32_t x = sorted[j];
+    if (j == 0 || sorted[j - 1] != x) seg_lo[x] = j;
+    if (j == n - 1 || sorted[j + 1] != x) seg_hi[x] = j + 1;
+}
+
+__global__ void k_segments_clear(uint32_t n, const uint32_t *sorted, uint32_t *seg_lo) {
+    uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < n) seg_lo[sorted[j]] = INVALID;
 }
 
 __global__ void k_sampling_unmark(uint32_t m, const uint32_t *dleaf, uint32_t *mark) {
@@ -342,7 +388,7 @@ __global__ void k_sampling_unmark(uint32_t m, const uint32_t *dleaf, uint32_t *m
 // Nodes::createNodesForSampling below the descent leaf (Nodes.cpp:285-336):
 // the chain of splits is a function of geometry only, since every node below
 // the first split is new.  Phase 0 counts splits, phase 1 materializes them.
-__global__ void k_sampling_apply(uint32_t m, const uint32_t *keys, const uint8_t *status, const uint8_t *unres,
+__global__ void k_sampling_apply(uint32_t m, const uint32_t *keys, const uint8_t *status, const uint32_t *unres,
                                  const uint32_t *dleaf, NV v, Root root, const D3 *pos, const D3 *nrm,
                                  const double *scale, double h_svo, uint32_t *nsplit, const uint32_t *base,
                                  uint32_t start, int phase, int *err) {
@@ -807,8 +853,8 @@ void sort_pairs(const K *kin, K *kout, const V *vin, V *vout, uint32_t n, cudaSt
     TSR_CUDA(cub::DeviceRadixSort::SortPairs(t.p, tmp, kin, kout, vin, vout, n, 0, end_bit, st));
 }
 
-template <class T>
-uint32_t select_flagged(const T *in, const uint8_t *flags, T *out, uint32_t n, cudaStream_t st) {
+template <class T, class F>
+uint32_t select_flagged(const T *in, const F *flags, T *out, uint32_t n, cudaStream_t st) {
     DBuf<uint32_t> cnt(1, st);
     size_t tmp = 0;
     TSR_CUDA(cub::DeviceSelect::Flagged(nullptr, tmp, in, flags, out, cnt.p, n, st));
@@ -817,7 +863,7 @@ uint32_t select_flagged(const T *in, const uint8_t *flags, T *out, uint32_t n, c
     return read_scalar(cnt.p, st);
 }
 
-__global__ void k_count_writers(uint32_t m, const uint8_t *status, const uint8_t *unres, unsigned long long *w) {
+__global__ void k_count_writers(uint32_t m, const uint8_t *status, const uint32_t *unres, unsigned long long *w) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < m && status[i] == 2 && !unres[i]) atomicAdd(w, 1ull);
 }
@@ -943,32 +989,72 @@ void build_tree(tsr_tree &t, const tsr_samples_view &sv, bool on_device) {
         uint32_t m = 2 * n;
         DBuf<uint32_t> keys(m, st), keys2(m, st);
         k_keys_init<<<grid_for(m, BLK), BLK, 0, st>>>(m, keys.p); ::tsr::note_launch();
-        DBuf<uint32_t> mark;
+        DBuf<uint32_t> mark, seg_lo, seg_hi;
         mark.alloc(S.cap, st);
         mark.fill_bytes(0xFF);
+        seg_lo.alloc(S.cap, st);
+        seg_lo.fill_bytes(0xFF);
+        seg_hi.alloc(S.cap, st);
         DBuf<unsigned long long> wcount(1, st);
         wcount.zero();
-        DBuf<uint32_t> changed(1, st);
-        uint32_t rounds = 0;
+        DBuf<uint32_t> counters(4, st);
+        uint32_t rounds = 0, waves = 0;
+        float eval_ms = 0, resolve_ms = 0;
+        cudaEvent_t e0, e1, e2;
+        TSR_CUDA(cudaEventCreate(&e0)); TSR_CUDA(cudaEventCreate(&e1)); TSR_CUDA(cudaEventCreate(&e2));
         while (m > 0) {
             if (++rounds > 100000) fail(TSR_ERR_TIMEOUT, "sampling rounds did not converge");
             NV v = view(S);
-            DBuf<uint8_t> status(m, st), unres(m, st);
-            DBuf<uint32_t> witness(m, st), dleaf(m, st);
+            DBuf<uint8_t> status(m, st);
+            DBuf<uint32_t> unres(m, st), witness(m, st), dleaf(m, st);
             unres.zero();
+            TSR_CUDA(cudaEventRecord(e0, st));
             k_sampling_eval<<<grid_for(m, 128), 128, 0, st>>>(m, keys.p, v, root, pos.p, nrm.p, scale.p, h_svo,
                                                              status.p, witness.p, dleaf.p, derr.p); ::tsr::note_launch();
-            if (int e0 = read_scalar(derr.p, st))
-                fail(TSR_ERR_DEVICE_ASSERT, "sampling evaluation invariant broken (code " + std::to_string(e0) + ")");
-            for (int it = 0;; ++it) {
-                if (it > 1000000) fail(TSR_ERR_TIMEOUT, "sampling conflict resolution did not converge");
-                changed.zero();
-                k_sampling_mark<<<grid_for(m, BLK), BLK, 0, st>>>(m, keys.p, status.p, unres.p, dleaf.p, mark.p); ::tsr::note_launch();
-                k_sampling_conflict<<<grid_for(m, 128), 128, 0, st>>>(m, keys.p, v, root, pos.p, nrm.p, scale.p, h_svo,
-                                                                     status.p, witness.p, dleaf.p, mark.p, unres.p,
-                                                                     changed.p, derr.p); ::tsr::note_launch();
-                if (read_scalar(changed.p, st) == 0) break;
+            TSR_CUDA(cudaEventRecord(e1, st));
+            if (int e0v = read_scalar(derr.p, st))
+                fail(TSR_ERR_DEVICE_ASSERT, "sampling evaluation invariant broken (code " + std::to_string(e0v) + ")");
+            // dependency index (leaf -> sides) and the writer list
+            DBuf<uint32_t> scnt(m + 1, st), soff(m + 1, st), writers(m, st);
+            TSR_CUDA(cudaMemsetAsync(scnt.p + m, 0, 4, st));
+            k_sens<<<grid_for(m, 128), 128, 0, st>>>(m, keys.p, v, root, pos.p, nrm.p, scale.p, h_svo, status.p,
+                                                    witness.p, dleaf.p, scnt.p, nullptr, nullptr, nullptr, 0,
+                                                    derr.p); ::tsr::note_launch();
+            exclusive_scan(scnt.p, soff.p, m + 1, st);
+            counters.zero();
+            k_writer_list<<<grid_for(m, BLK), BLK, 0, st>>>(m, status.p, writers.p, counters.p); ::tsr::note_launch();
+            uint32_t cnt[2];
+            TSR_CUDA(cudaMemcpyAsync(&cnt[0], soff.p + m, 4, cudaMemcpyDeviceToHost, st));
+            TSR_CUDA(cudaMemcpyAsync(&cnt[1], counters.p, 4, cudaMemcpyDeviceToHost, st));
+            TSR_CUDA(cudaStreamSynchronize(st));
+            const uint32_t nsens = cnt[0], nwri = cnt[1];
+            DBuf<uint32_t> skeys(nsens, st), svals(nsens, st), ssorted(nsens, st), by_leaf(nsens, st);
+            if (nsens) {
+                k_sens<<<grid_for(m, 128), 128, 0, st>>>(m, keys.p, v, root, pos.p, nrm.p, scale.p, h_svo, status.p,
+                                                        witness.p, dleaf.p, nullptr, soff.p, skeys.p, svals.p, 1,
+                                                        derr.p); ::tsr::note_launch();
+                sort_pairs(skeys.p, ssorted.p, svals.p, by_leaf.p, nsens, st);
+                k_segments<<<grid_for(nsens, BLK), BLK, 0, st>>>(nsens, ssorted.p, seg_lo.p, seg_hi.p); ::tsr::note_launch();
             }
+            // waves: the frontier starts with every writer
+            DBuf<uint32_t> front(m, st), next(m, st), touched(m, st);
+            uint32_t nf = nwri;
+            if (nwri) TSR_CUDA(cudaMemcpyAsync(front.p, writers.p, (size_t)nwri * 4, cudaMemcpyDeviceToDevice, st));
+            while (nf > 0) {
+                if (++waves > 10000000) fail(TSR_ERR_TIMEOUT, "sampling conflict resolution did not converge");
+                TSR_CUDA(cudaMemsetAsync(counters.p, 0, 8, st));
+                k_wave_mark<<<grid_for(nf, BLK), BLK, 0, st>>>(nf, front.p, keys.p, dleaf.p, mark.p, touched.p,
+                                                              counters.p); ::tsr::note_launch();
+                uint32_t nt = read_scalar(counters.p, st);
+                if (nt == 0) break;
+                k_wave_witness<<<grid_for((size_t)nt * 32, BLK), BLK, 0, st>>>(nt, touched.p, seg_lo.p, seg_hi.p,
+                                                                             by_leaf.p, keys.p, mark.p, unres.p,
+                                                                             next.p, counters.p + 1); ::tsr::note_launch();
+                nf = read_scalar(counters.p + 1, st);
+                std::swap(front, next);
+            }
+            TSR_CUDA(cudaEventRecord(e2, st));
+            if (nsens) k_segments_clear<<<grid_for(nsens, BLK), BLK, 0, st>>>(nsens, ssorted.p, seg_lo.p); ::tsr::note_launch();
             k_count_writers<<<grid_for(m, BLK), BLK, 0, st>>>(m, status.p, unres.p, wcount.p); ::tsr::note_launch();
             // commit resolved writers
             DBuf<uint32_t> nsplit(m + 1, st), base(m + 1, st);
@@ -977,14 +1063,22 @@ void build_tree(tsr_tree &t, const tsr_samples_view &sv, bool on_device) {
                                                               nrm.p, scale.p, h_svo, nsplit.p, nullptr, 0, 0, derr.p); ::tsr::note_launch();
             exclusive_scan(nsplit.p, base.p, m + 1, st);
             uint32_t total = read_scalar(base.p + m, st);
+            float a = 0, b = 0;
+            TSR_CUDA(cudaEventElapsedTime(&a, e0, e1));
+            TSR_CUDA(cudaEventElapsedTime(&b, e1, e2));
+            eval_ms += a;
+            resolve_ms += b;
             if (total) {
                 uint32_t old_cap = S.cap;
                 S.ensure((uint64_t)S.count + 8ull * total);
                 if (S.cap != old_cap) {
-                    DBuf<uint32_t> nm(S.cap, st);
-                    nm.fill_bytes(0xFF);
-                    TSR_CUDA(cudaMemcpyAsync(nm.p, mark.p, (size_t)old_cap * 4, cudaMemcpyDeviceToDevice, st));
-                    mark = std::move(nm);
+                    for (DBuf<uint32_t> *arr : {&mark, &seg_lo}) {
+                        DBuf<uint32_t> nm(S.cap, st);
+                        nm.fill_bytes(0xFF);
+                        TSR_CUDA(cudaMemcpyAsync(nm.p, arr->p, (size_t)old_cap * 4, cudaMemcpyDeviceToDevice, st));
+                        *arr = std::move(nm);
+                    }
+                    seg_hi.alloc(S.cap, st);
                 }
                 v = view(S);
                 k_sampling_apply<<<grid_for(m, 128), 128, 0, st>>>(m, keys.p, status.p, unres.p, dleaf.p, v, root,
@@ -998,7 +1092,11 @@ void build_tree(tsr_tree &t, const tsr_samples_view &sv, bool on_device) {
             std::swap(keys, keys2);
             m = m2;
         }
+        cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(e2);
         t.sampling_rounds = rounds;
+        t.sampling_waves = waves;
+        t.stage_ms[6] = eval_ms;
+        t.stage_ms[7] = resolve_ms;
         t.sampling_writers = read_scalar(wcount.p, st);
         int e = read_scalar(derr.p, st);
         if (e) fail(TSR_ERR_DEVICE_ASSERT, "sampling traversal invariant broken (code " + std::to_string(e) + ")");
