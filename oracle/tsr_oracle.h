@@ -17,9 +17,16 @@
  * this path, and its geometry helpers (BaseProject's ObliqueCircularCone,
  * intersectAABBWithSphere, intersectAABBWithLineSegment, Plane, EPSILON) are
  * not in the reference tree.  Those helpers are restated here from their call
- * sites; parity at that boundary is UNPINNED.  The tree/leaves/dual-cell and
- * DMC code paths are additionally checked against the reference's own sources
- * compiled with a stand-in for the absent BaseProject headers (oracle/ref_shim).
+ * sites; PARITY UNPINNED: the reference's own sources cannot be compiled
+ * here (they need the absent BaseProject library and its cmake build), so no
+ * reference-produced output backs this restatement.  What pins it instead is
+ * structural: the tests check the restatement's invariants (every sample
+ * inside its container, consistent parent/child links, the block-DFS node
+ * layout, leaves partitioning the root with the depth-difference balance,
+ * dual cells built from existing leaves, the Marching Cubes tables, well
+ * formed meshes, the round schedule equal to the sequential sampling pass,
+ * cone pruning leaving the kernel sums unchanged) and replay its committed
+ * golden fixtures.
  */
 #ifndef TSR_ORACLE_H
 #define TSR_ORACLE_H

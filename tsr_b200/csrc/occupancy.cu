@@ -295,7 +295,8 @@ __device__ inline bool cone_box_separated_pt(const ConeF &c, F3 bmin, float size
 constexpr int PT_BLOCK = 128;
 
 template <int TYPE>
-__global__ void __launch_bounds__(PT_BLOCK) k_cone_pt(uint64_t nlinks, const uint32_t *order, LinkIn in, TreeIn tr,
+__global__ void __launch_bounds__(PT_BLOCK, (TYPE == 0) ? 6 : 5) k_cone_pt(uint64_t nlinks, const uint32_t *order, LinkIn in, TreeIn tr,
+                                                         const uint2 *cs,
                                                       uint32_t *states, float2 *ksum, float2 *clen,
                                                       double *cone_count, unsigned long long *accepted,
                                                       unsigned long long *next_link, unsigned long long *visits,
@@ -441,8 +442,9 @@ __global__ void __launch_bounds__(PT_BLOCK) k_cone_pt(uint64_t nlinks, const uin
                 float size = ldexpf(root_size_f, -(int)d);
                 F3 bmin = f3((ci & 1u) ? top_min.x + size : top_min.x, (ci & 2u) ? top_min.y + size : top_min.y,
                              (ci & 4u) ? top_min.z + size : top_min.z);
-                if (!(req && (states[idx] & req) != req)) {
-                    uint32_t cc0 = tr.children[idx];
+                uint2 rec = cs[idx];   // (children, state) in one load
+                if (!(req && (rec.y & req) != req)) {
+                    uint32_t cc0 = rec.x;
                     if (cc0 == INVALID) {
                         // a leaf: addKernel's exact test decides, no box test needed
                         visit_leaf(idx, bmin, size);
@@ -475,6 +477,12 @@ __global__ void __launch_bounds__(PT_BLOCK) k_cone_pt(uint64_t nlinks, const uin
         if (acc) atomicAdd(accepted, acc);
         if (nvis) atomicAdd(visits, nvis);
     }
+}
+
+// (child block, state word) per node, read with one load by the traversals.
+__global__ void k_pack_cs(uint32_t nn, const uint32_t *children, const uint32_t *states, uint2 *out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nn) out[i] = make_uint2(children[i], states ? states[i] : 0u);
 }
 
 __global__ void k_link_cameras(uint64_t nlinks, const uint32_t *links, uint32_t ncams, uint32_t *keys,
@@ -732,12 +740,14 @@ void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_
     // traversal and results, no persistent scheduling) for comparisons
     const char *kenv = getenv("TSR_CONE_KERNEL");
     const bool per_thread = kenv && kenv[0] == 't';
+    DBuf<uint2> packed(nn, st);
+    k_pack_cs<<<grid_for(nn, BLK), BLK, 0, st>>>(nn, t.children.p, nullptr, packed.p); ::tsr::note_launch();
     if (per_thread) {
         k_cone_pass<SAMPLENESS><<<grid, 128, 0, st>>>(nlinks, in, tr, o.states.p, ssum, slen, cone_count.p,
                                                       accepted.p + 1, err.p);
     } else {
         next_link.zero();
-        k_cone_pt<SAMPLENESS><<<pt_grid, PT_BLOCK, 0, st>>>(nlinks, nullptr, in, tr, o.states.p, ssum, slen,
+        k_cone_pt<SAMPLENESS><<<pt_grid, PT_BLOCK, 0, st>>>(nlinks, nullptr, in, tr, packed.p, o.states.p, ssum, slen,
                                                            cone_count.p, accepted.p + 1, next_link.p,
                                                            accepted.p + 3, err.p);
     }
@@ -762,13 +772,14 @@ void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_
         k_forward_flag<<<grid_for(hi - lo, BLK), BLK, 0, st>>>(lo, hi, t.level_order.p, t.children.p, o.states.p,
                                                               FLAG_SAMPLENESS); ::tsr::note_launch();
     }
+    k_pack_cs<<<grid_for(nn, BLK), BLK, 0, st>>>(nn, t.children.p, o.states.p, packed.p); ::tsr::note_launch();
     o.stage_ms[1] = timer.lap();
     if (per_thread) {
         k_cone_pass<EMPTINESS><<<grid, 128, 0, st>>>(nlinks, in, tr, o.states.p, esum, elen, cone_count.p, accepted.p,
                                                      err.p);
     } else {
         next_link.zero();
-        k_cone_pt<EMPTINESS><<<pt_grid, PT_BLOCK, 0, st>>>(nlinks, order.p, in, tr, o.states.p, esum, elen,
+        k_cone_pt<EMPTINESS><<<pt_grid, PT_BLOCK, 0, st>>>(nlinks, order.p, in, tr, packed.p, o.states.p, esum, elen,
                                                           cone_count.p, accepted.p, next_link.p, accepted.p + 2,
                                                           err.p);
     }

@@ -12,12 +12,15 @@
 // here and nothing else.  Node storage indices during the build follow
 // allocation order; the relayout at the end maps them onto the reference's
 // block-DFS numbering, which depends only on topology.
+#include <cooperative_groups.h>
 #include <cub/cub.cuh>
 
 #include <algorithm>
 #include <vector>
 
 #include "handles.h"
+
+namespace cg = cooperative_groups;
 
 namespace tsr {
 namespace {
@@ -306,33 +309,58 @@ __global__ void k_sampling_eval(uint32_t m, const uint32_t *keys, NV v, Root roo
 // wave from the writers.  The result is the least fixed point, i.e. exactly
 // what a sequential pass in key order computes.
 
-// Wave members claim their descent leaf; leaves whose claim dropped are
-// recorded for the witness scan.
-__global__ void k_wave_mark(uint32_t nf, const uint32_t *frontier, const uint32_t *keys, const uint32_t *dleaf,
-                            uint32_t *mark, uint32_t *touched, uint32_t *ntouched) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nf) return;
-    uint32_t p = frontier[i];
-    uint32_t x = dleaf[p], k = keys[p];
-    uint32_t old = atomicMin(&mark[x], k);
-    if (old > k) touched[atomicAdd(ntouched, 1u)] = x;
-}
-
-// Reliable sides witnessed by a leaf claimed by an earlier key become
-// unresolved (one warp per touched leaf).
-__global__ void k_wave_witness(uint32_t nt, const uint32_t *touched, const uint32_t *seg_lo, const uint32_t *seg_hi,
-                               const uint32_t *by_witness, const uint32_t *keys, const uint32_t *mark,
-                               uint32_t *unres, uint32_t *next, uint32_t *nnext) {
-    uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (w >= nt) return;
-    uint32_t x = touched[w];
-    uint32_t lo = seg_lo[x];
-    if (lo == INVALID) return;
-    uint32_t hi = seg_hi[x], mk = mark[x];
-    for (uint32_t j = lo + lane; j < hi; j += 32) {
-        uint32_t q = by_witness[j];
-        if (keys[q] > mk && atomicExch(&unres[q], 1u) == 0u) next[atomicAdd(nnext, 1u)] = q;
+// Each wave: members claim their descent leaf with their key (leaves whose
+// claim dropped are recorded), then every side depending on a recorded leaf
+// with a larger key becomes unresolved and joins the next wave.
+//
+// All waves of one round in one cooperative launch (grid-wide barriers
+// instead of a host round trip per wave).  Counter pairs alternate by wave
+// parity; the idle pair is cleared between the two barriers of a wave, when
+// no thread can still be reading it.  The wave count is bounded.
+__global__ void k_waves_coop(uint32_t nf0, uint32_t *front, uint32_t *next, const uint32_t *keys,
+                             const uint32_t *dleaf, uint32_t *mark, uint32_t *touched, const uint32_t *seg_lo,
+                             const uint32_t *seg_hi, const uint32_t *by_leaf, uint32_t *unres, uint32_t *ctr,
+                             uint32_t max_waves, uint32_t *waves_out, int *err) {
+    cg::grid_group grid = cg::this_grid();
+    const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t gsize = gridDim.x * blockDim.x;
+    const uint32_t lane = threadIdx.x & 31, gwarp = gtid >> 5, nwarps = gsize >> 5;
+    uint32_t nf = nf0;
+    uint32_t wave = 0;
+    while (nf > 0) {
+        if (wave >= max_waves) {
+            if (gtid == 0) atomicExch(err, 7);
+            break;
+        }
+        uint32_t *c = ctr + 2 * (wave & 1);        // this wave's (touched, next) counters
+        uint32_t *c_idle = ctr + 2 * ((wave + 1) & 1);
+        for (uint32_t i = gtid; i < nf; i += gsize) {
+            uint32_t p = front[i];
+            uint32_t x = dleaf[p], k = keys[p];
+            uint32_t old = atomicMin(&mark[x], k);
+            if (old > k) touched[atomicAdd(&c[0], 1u)] = x;
+        }
+        grid.sync();
+        if (gtid == 0) { c_idle[0] = 0; c_idle[1] = 0; }
+        const uint32_t nt = c[0];
+        for (uint32_t j = gwarp; j < nt; j += nwarps) {
+            uint32_t x = touched[j];
+            uint32_t lo = seg_lo[x];
+            if (lo == INVALID) continue;
+            uint32_t hi = seg_hi[x], mk = mark[x];
+            for (uint32_t q2 = lo + lane; q2 < hi; q2 += 32) {
+                uint32_t q = by_leaf[q2];
+                if (keys[q] > mk && atomicExch(&unres[q], 1u) == 0u) next[atomicAdd(&c[1], 1u)] = q;
+            }
+        }
+        grid.sync();
+        nf = c[1];
+        uint32_t *tmp = front;
+        front = next;
+        next = tmp;
+        ++wave;
     }
+    if (gtid == 0) *waves_out = wave;
 }
 
 // Dependency lists: the leaves each pending side depends on (its witness if
@@ -1002,6 +1030,14 @@ void build_tree(tsr_tree &t, const tsr_samples_view &sv, bool on_device) {
         float eval_ms = 0, resolve_ms = 0;
         cudaEvent_t e0, e1, e2;
         TSR_CUDA(cudaEventCreate(&e0)); TSR_CUDA(cudaEventCreate(&e1)); TSR_CUDA(cudaEventCreate(&e2));
+        unsigned coop_grid = 1;
+        {
+            int dev = 0, sms = 0, per_sm = 0;
+            TSR_CUDA(cudaGetDevice(&dev));
+            TSR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+            TSR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_waves_coop, 256, 0));
+            coop_grid = (unsigned)(sms * (per_sm > 0 ? per_sm : 1));
+        }
         while (m > 0) {
             if (++rounds > 100000) fail(TSR_ERR_TIMEOUT, "sampling rounds did not converge");
             NV v = view(S);
@@ -1039,19 +1075,20 @@ void build_tree(tsr_tree &t, const tsr_samples_view &sv, bool on_device) {
             // waves: the frontier starts with every writer
             DBuf<uint32_t> front(m, st), next(m, st), touched(m, st);
             uint32_t nf = nwri;
-            if (nwri) TSR_CUDA(cudaMemcpyAsync(front.p, writers.p, (size_t)nwri * 4, cudaMemcpyDeviceToDevice, st));
-            while (nf > 0) {
-                if (++waves > 10000000) fail(TSR_ERR_TIMEOUT, "sampling conflict resolution did not converge");
-                TSR_CUDA(cudaMemsetAsync(counters.p, 0, 8, st));
-                k_wave_mark<<<grid_for(nf, BLK), BLK, 0, st>>>(nf, front.p, keys.p, dleaf.p, mark.p, touched.p,
-                                                              counters.p); ::tsr::note_launch();
-                uint32_t nt = read_scalar(counters.p, st);
-                if (nt == 0) break;
-                k_wave_witness<<<grid_for((size_t)nt * 32, BLK), BLK, 0, st>>>(nt, touched.p, seg_lo.p, seg_hi.p,
-                                                                             by_leaf.p, keys.p, mark.p, unres.p,
-                                                                             next.p, counters.p + 1); ::tsr::note_launch();
-                nf = read_scalar(counters.p + 1, st);
-                std::swap(front, next);
+            if (nwri) {
+                TSR_CUDA(cudaMemcpyAsync(front.p, writers.p, (size_t)nwri * 4, cudaMemcpyDeviceToDevice, st));
+                DBuf<uint32_t> ctr(4, st), waves_out(1, st);
+                ctr.zero();
+                uint32_t max_waves = 1u << 22;
+                uint32_t *fp = front.p, *np = next.p, *tp = touched.p, *kp = keys.p, *dp = dleaf.p, *mp = mark.p;
+                uint32_t *slp = seg_lo.p, *shp = seg_hi.p, *blp = by_leaf.p, *up = unres.p, *cp = ctr.p;
+                uint32_t *wp = waves_out.p;
+                int *ep = derr.p;
+                void *args[] = {&nf, &fp, &np, &kp, &dp, &mp, &tp, &slp, &shp, &blp, &up, &cp, &max_waves, &wp, &ep};
+                TSR_CUDA(cudaLaunchCooperativeKernel((const void *)k_waves_coop, coop_grid, 256, args, 0, st));
+                ::tsr::note_launch();
+                waves += read_scalar(waves_out.p, st);
+                if (read_scalar(derr.p, st) == 7) fail(TSR_ERR_TIMEOUT, "sampling conflict resolution did not converge");
             }
             TSR_CUDA(cudaEventRecord(e2, st));
             if (nsens) k_segments_clear<<<grid_for(nsens, BLK), BLK, 0, st>>>(nsens, ssorted.p, seg_lo.p); ::tsr::note_launch();
