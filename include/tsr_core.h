@@ -136,6 +136,22 @@ TSR_API tsr_status tsr_tree_build_device(const tsr_samples_view *samples, const 
 TSR_API void tsr_tree_free(tsr_tree *tree);
 TSR_API tsr_status tsr_tree_get_counts(const tsr_tree *tree, tsr_tree_counts *out);
 TSR_API tsr_status tsr_tree_root_scope(const tsr_tree *tree, double min_xyz_size[4]);
+/* The root scope tsr_tree_build would give these samples (min corner xyz and
+ * edge length of the root cube, as tsr_tree_root_scope reports), written to
+ * DEVICE memory `out_min_xyz_size[4]` on `cuda_stream`, with DEVICE inputs
+ * (`positions` 3 * count xyz-interleaved, `scales` count).  No counterpart in
+ * the reference: it exists for callers that must not allocate (their device
+ * memory is all handed to their own pool, or their footprint is fixed after
+ * start-up).  It allocates no memory; its working memory is a fixed 56,836 B
+ * array per device inside the library.  The first call on each device sets
+ * that up (address look-up, which may load the library's device code), so
+ * make it before any stream capture.  Calls on one device share the array:
+ * calls that may overlap in time race, so order them.  count must be
+ * 1 .. 2^32 - 1 (TSR_ERR_OVERFLOW_U32 above); pointers must be 8-byte aligned
+ * memory of the current device. */
+TSR_API tsr_status tsr_samples_root_scope_noalloc(uint64_t count, const double *positions,
+                                                  const double *scales, const tsr_params *params,
+                                                  double *out_min_xyz_size, void *cuda_stream);
 /* Node arrays after the reference's reorder; any pointer may be NULL. */
 TSR_API tsr_status tsr_tree_copy_nodes(const tsr_tree *tree, uint32_t *children, uint32_t *parents,
                                uint32_t *sample_counts, uint32_t *sample_starts);

@@ -74,6 +74,7 @@ _sig = {
     "tsr_tree_free": (None, [_P]),
     "tsr_tree_get_counts": (ctypes.c_int, [_P, _P]),
     "tsr_tree_root_scope": (ctypes.c_int, [_P, _P]),
+    "tsr_samples_root_scope_noalloc": (ctypes.c_int, [ctypes.c_uint64, _P, _P, _P, _P, _P]),
     "tsr_tree_copy_nodes": (ctypes.c_int, [_P, _P, _P, _P, _P]),
     "tsr_tree_copy_permutation": (ctypes.c_int, [_P, _P]),
     "tsr_tree_copy_leaves": (ctypes.c_int, [_P, _P, _P, _P, _P, _P]),

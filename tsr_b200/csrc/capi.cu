@@ -162,6 +162,15 @@ tsr_status tsr_tree_root_scope(const tsr_tree *t, double m[4]) {
     });
 }
 
+tsr_status tsr_samples_root_scope_noalloc(uint64_t count, const double *positions, const double *scales,
+                                          const tsr_params *params, double *out_min_xyz_size, void *cuda_stream) {
+    return guarded([&] {
+        if (!params) fail(TSR_ERR_INVALID_ARG, "null argument");
+        root_scope_noalloc(count, positions, scales, params->max_relative_sampling_distance, out_min_xyz_size,
+                           static_cast<cudaStream_t>(cuda_stream));
+    });
+}
+
 tsr_status tsr_tree_copy_nodes(const tsr_tree *t, uint32_t *children, uint32_t *parents, uint32_t *sample_counts,
                                uint32_t *sample_starts) {
     return guarded([&] {

@@ -60,4 +60,6 @@ void build_tree(tsr_tree &t, const tsr_samples_view &sv, bool on_device);
 void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_params &p, int mode,
                        tsr_occupancy &o);
 void extract_dmc(const tsr_tree &t, const tsr_occupancy &o, tsr_mesh &m);
+void root_scope_noalloc(uint64_t count, const double *positions, const double *scales, double h_svo,
+                        double *out_min_xyz_size, cudaStream_t st);
 }  // namespace tsr
