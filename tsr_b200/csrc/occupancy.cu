@@ -56,39 +56,9 @@ struct LinkIn {
 };
 
 struct TreeIn {
-    const uint32_t *children;
-    const uint8_t *depth;
-    const D3 *nmin;
-    const uint32_t *node_to_leaf;
+    const D3 *nmin;   // node min corners (FP64), for the start-node descent
 };
 
-__device__ inline void add_comp(float2 *slot, float v) {
-    float old = atomicAdd(&slot->x, v);
-    float s = old + v;
-    float bp = s - old;
-    float err = (old - (s - bp)) + (v - bp);
-    if (err != 0.0f) atomicAdd(&slot->y, err);
-}
-
-// Conservative cone/box rejection (stands in for ObliqueCircularCone::
-// haveSeparatingAxis, ConeNodesChecker.cpp:65).  Pruning can only skip boxes
-// that contain no point of the cut cone, so the sums do not depend on it.
-__device__ inline bool cone_box_separated(const ConeF &c, F3 bmin, float size) {
-    float h = 0.5f * size;
-    F3 ctr = bmin + f3(h, h, h);
-    F3 u = ctr - c.end;
-    float te = fdot(u, c.m) * c.inv_denom;
-    float dt = h * c.n1 * fabsf(c.inv_denom);
-    float slack = 1e-4f * (dt + fabsf(te)) + 1e-6f;
-    if (te + dt < c.t_start_e - slack) return true;
-    if (te - dt >= slack) return true;
-    if (1.0f + te + dt <= 0.0f) return true;
-    F3 q = u - c.axis * te;
-    float qn = sqrtf(fdot(q, q));
-    float tmax = fminf(1.0f + te + dt, 1.0f);
-    float bound = qn - h * 1.7320508f - dt * c.full;
-    return bound > tmax * c.radius * 1.0001f + 1e-4f * (qn + h + dt * c.full);
-}
 
 // Occupancy::addKernel (Occupancy.cpp:279-346) at leaf centre x.
 __device__ inline bool eval_kernel(const ConeF &c, F3 x, bool sampleness, float conf, float *out) {
@@ -127,151 +97,10 @@ __device__ inline F3 rel(const D3 &a, const D3 &origin) {
     return f3((float)(a.x - origin.x), (float)(a.y - origin.y), (float)(a.z - origin.z));
 }
 
-// One thread per camera-to-sample link (Occupancy.cpp:170-236).
-template <int TYPE>
-__global__ void __launch_bounds__(128) k_cone_pass(uint64_t nlinks, LinkIn in, TreeIn tr, uint32_t *states,
-                                                   float2 *ksum, float2 *clen, double *cone_count,
-                                                   unsigned long long *accepted, int *err) {
-    uint64_t l = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    double count = 0.0;
-    unsigned long long acc = 0;
-    if (l < nlinks) do {
-        uint32_t s = (uint32_t)(l / in.k);
-        uint32_t cam = in.links[l];
-        if (cam == INVALID || cam >= in.ncams) break;
-        D3 p = in.pos[s];
-        D3 n = in.nrm[s];
-        D3 cw = in.cams[cam];
-        double kernel_r = in.h_o * in.scale[s];
-        // FP64 cone set-up (Occupancy.cpp:180-201)
-        D3 apex_d{cw.x - p.x, cw.y - p.y, cw.z - p.z};   // apex relative to the sample
-        D3 end_d{0.0, 0.0, 0.0};
-        double cone_len = REAL_MAX;
-        if (TYPE == SAMPLENESS) {
-            D3 cs{-apex_d.x, -apex_d.y, -apex_d.z};
-            double total = sqrt(cs.x * cs.x + cs.y * cs.y + cs.z * cs.z);
-            cone_len = kernel_r * in.rel_cone;
-            double h = cone_len * 0.5;
-            end_d = D3{cs.x / total * h, cs.y / total * h, cs.z / total * h};
-        }
-        D3 m{-n.x, -n.y, -n.z};
-        D3 axis{end_d.x - apex_d.x, end_d.y - apex_d.y, end_d.z - apex_d.z};
-        double full = sqrt(axis.x * axis.x + axis.y * axis.y + axis.z * axis.z);
-        double length = cone_len < full ? cone_len : full;
-        double denom = axis.x * m.x + axis.y * m.y + axis.z * m.z;
-        if (!(full > EPS) || !(kernel_r > 0.0) || fabs(denom) <= EPS * full) break;   // isDegenerated
-        double conf = in.conf[s];
-        if (TYPE == EMPTINESS) count = conf;
-        float wlen = (float)(conf * length);
-        double depth_d = ceil(log2(in.root_size / (in.scale[s] * in.h_svo)));   // Tree.cpp:86-91
-        uint32_t max_depth = (uint32_t)depth_d + MAX_DEPTH_DIFFERENCE;
-        ConeF c;
-        c.apex = f3((float)apex_d.x, (float)apex_d.y, (float)apex_d.z);
-        c.end = f3((float)end_d.x, (float)end_d.y, (float)end_d.z);
-        c.axis = f3((float)axis.x, (float)axis.y, (float)axis.z);
-        c.m = f3((float)m.x, (float)m.y, (float)m.z);
-        c.radius = (float)kernel_r;
-        c.full = (float)full;
-        c.length = (float)length;
-        c.inv_denom = (float)(1.0 / denom);
-        c.a_over_l = (float)(full / length);
-        c.t_start_e = (float)(-length / full);   // tComplete - 1 at the cut start
-        c.n1 = fabsf(c.m.x) + fabsf(c.m.y) + fabsf(c.m.z);
-        const float fconf = (float)conf;
-        const uint32_t req = (TYPE == EMPTINESS) ? FLAG_SAMPLENESS : 0u;
-        const uint32_t leaf_flag = (TYPE == EMPTINESS) ? FLAG_EMPTINESS : FLAG_SAMPLENESS;
-        const float root_size_f = (float)in.root_size;
-
-        // LeavesIterator with ConeNodesChecker (NodesIterator.cpp:38-86)
-        auto ignored = [&](uint32_t node, F3 bmin, float size) -> bool {
-            if (req && (states[node] & req) != req) return true;
-            return cone_box_separated(c, bmin, size);
-        };
-        auto visit_leaf = [&](uint32_t node, F3 bmin, float size) {
-            float h = 0.5f * size;
-            float val;
-            if (!eval_kernel(c, bmin + f3(h, h, h), TYPE == SAMPLENESS, fconf, &val)) return;
-            uint32_t leaf = tr.node_to_leaf[node];
-            add_comp(&ksum[leaf], val);
-            add_comp(&clen[leaf], wlen);
-            if ((states[node] & leaf_flag) == 0) atomicOr(&states[node], leaf_flag);
-            ++acc;
-        };
-        // Start at the deepest node that contains the cut cone's bounding box
-        // (the capsule of radius R around the cut axis): every ancestor then
-        // contains the whole cone, so none of them can be pruned, and no leaf
-        // outside it can hold a point of the cone.
-        F3 p0 = c.end + c.axis * c.t_start_e;
-        F3 lo = f3(fminf(p0.x, c.end.x) - c.radius, fminf(p0.y, c.end.y) - c.radius, fminf(p0.z, c.end.z) - c.radius);
-        F3 hi = f3(fmaxf(p0.x, c.end.x) + c.radius, fmaxf(p0.y, c.end.y) + c.radius, fmaxf(p0.z, c.end.z) + c.radius);
-        uint32_t start = 0, base = 0;
-        F3 smin = rel(tr.nmin[0], p);
-        float ssize = root_size_f;
-        while (tr.children[start] != INVALID && base + 1 <= max_depth) {
-            float cs = 0.5f * ssize;
-            float margin = 1e-5f * ssize;
-            F3 ctr = smin + f3(cs, cs, cs);
-            uint32_t digit = 0;
-            bool inside = true;
-            const float l3[3] = {lo.x, lo.y, lo.z}, h3[3] = {hi.x, hi.y, hi.z}, c3[3] = {ctr.x, ctr.y, ctr.z};
-            for (int a = 0; a < 3; ++a) {
-                if (h3[a] < c3[a] - margin) continue;
-                if (l3[a] > c3[a] + margin) { digit |= 1u << a; continue; }
-                inside = false;
-            }
-            if (!inside) break;
-            start = tr.children[start] + digit;
-            smin = rel(tr.nmin[start], p);
-            ssize = cs;
-            ++base;
-        }
-        if (ignored(start, smin, ssize)) break;
-        if (tr.children[start] == INVALID) { visit_leaf(start, smin, ssize); break; }
-        if (base + 1 > max_depth) break;
-        uint32_t st_node[MAX_TREE_DEPTH];
-        uint8_t st_next[MAX_TREE_DEPTH];
-        int sp = 1;
-        st_node[0] = start;
-        st_next[0] = 0;
-        while (sp > 0) {
-            int t = sp - 1;
-            if (st_next[t] == 8) { --sp; continue; }
-            uint32_t ci = st_next[t]++;
-            uint32_t idx = tr.children[st_node[t]] + ci;
-            uint32_t d = base + (uint32_t)t + 1;   // depth of the child
-            float size = ldexpf(root_size_f, -(int)d);
-            F3 bmin = rel(tr.nmin[idx], p);
-            if (ignored(idx, bmin, size)) continue;
-            if (tr.children[idx] == INVALID) { visit_leaf(idx, bmin, size); continue; }
-            if (d + 1 > max_depth) continue;   // goDown stops at the depth cap
-            if (sp >= MAX_TREE_DEPTH) { atomicExch(err, 1); break; }
-            st_node[sp] = idx;
-            st_next[sp] = 0;
-            ++sp;
-        }
-    } while (0);
-    // block-level reduction of the cone count and the accepted counter
-    typedef cub::BlockReduce<double, 128> BR;
-    typedef cub::BlockReduce<unsigned long long, 128> BRU;
-    __shared__ typename BR::TempStorage tmp;
-    __shared__ typename BRU::TempStorage tmpu;
-    double bc = BR(tmp).Sum(count);
-    unsigned long long ba = BRU(tmpu).Sum(acc);
-    if (threadIdx.x == 0) {
-        if (TYPE == EMPTINESS && bc != 0.0) atomicAdd(cone_count, bc);
-        if (ba) atomicAdd(accepted, ba);
-    }
-}
-
-// ---------------------------------------------- persistent cone traversal
-// Thread-per-link depth-first traversal (the per-link LeavesIterator with a
-// ConeNodesChecker) run by persistent threads: a lane whose traversal ends
-// immediately takes the next link, fetched per warp in one atomic batch, so
-// lanes do not idle behind the warp's longest link.  Child boxes are derived
-// from the parent's box in the link's FP32 frame (no node-geometry loads
-// inside the loop); node records read per visit are the child block index and,
-// for EMPTINESS, the state word.
-
+// ------------------------------------------------------ cone traversal
+// Conservative cone/box rejection (stands in for ObliqueCircularCone::
+// haveSeparatingAxis, ConeNodesChecker.cpp:65).  Pruning can only skip boxes
+// that contain no point of the cut cone, so the sums do not depend on it.
 // Conservative box test with an absolute slack for the FP32 box recurrence.
 __device__ inline bool cone_box_separated_pt(const ConeF &c, F3 bmin, float size) {
     float h = 0.5f * size;
@@ -294,44 +123,93 @@ __device__ inline bool cone_box_separated_pt(const ConeF &c, F3 bmin, float size
 
 constexpr int PT_BLOCK = 128;
 
+// ------------------------------------------- block-expansion cone traversal
+// Thread-per-link depth-first traversal (the per-link LeavesIterator with a
+// ConeNodesChecker) run by persistent threads: a lane whose traversal ends
+// takes the next link, fetched per warp in one atomic batch, so lanes do not
+// idle behind the warp's longest link.  Child boxes are derived from the
+// parent's box in the link's FP32 frame.  The traversal is organised around
+// children blocks: every step expands one node, loading its eight children's records in one 64-byte
+// line and testing all eight at once, then descends straight into the first
+// surviving child; only nodes with further surviving children go on the
+// stack.  One dependent load per expanded node replaces one per visited
+// child.  Leaf flags are not written here: a leaf got a kernel exactly when
+// its sum is non-zero (every accepted value is >= EPSILON), so they are set
+// afterwards from the sums.
+//
+// Node records: rec[i + 7] = (first child or INVALID, leaf index or
+// REC_NOLEAF, with the node's SAMPLENESS flag in bit 31).  Children blocks
+// start at 1 + 8k (root 0, then whole blocks of 8), so a block's records
+// start on a 64-byte boundary.
+constexpr uint32_t REC_FLAG = 0x80000000u, REC_NOLEAF = 0x7FFFFFFFu;
+constexpr uint32_t REC_OFFSET = 7;
+
+__global__ void k_pack_rec(uint32_t nn, const uint32_t *children, const uint32_t *node_to_leaf,
+                           const uint32_t *states, uint2 *rec) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nn) return;
+    uint32_t c = children[i];
+    uint32_t y = (c == INVALID) ? node_to_leaf[i] : REC_NOLEAF;
+    if (states && (states[i] & FLAG_SAMPLENESS)) y |= REC_FLAG;
+    rec[i + REC_OFFSET] = make_uint2(c, y);
+}
+
+__device__ __forceinline__ F3 child_min(F3 pmin, uint32_t ci, float size) {
+    return f3((ci & 1u) ? pmin.x + size : pmin.x, (ci & 2u) ? pmin.y + size : pmin.y,
+              (ci & 4u) ? pmin.z + size : pmin.z);
+}
+
 template <int TYPE>
-__global__ void __launch_bounds__(PT_BLOCK, (TYPE == 0) ? 6 : 5) k_cone_pt(uint64_t nlinks, const uint32_t *order, LinkIn in, TreeIn tr,
-                                                         const uint2 *cs,
-                                                      uint32_t *states, float2 *ksum, float2 *clen,
-                                                      double *cone_count, unsigned long long *accepted,
-                                                      unsigned long long *next_link, unsigned long long *visits,
-                                                      int *err) {
+__global__ void __launch_bounds__(PT_BLOCK, (TYPE == 0) ? 6 : 5) k_cone_x(uint64_t nlinks, const uint32_t *order, LinkIn in,
+                                                        TreeIn tr, const uint2 *rec, double *ksum, double *clen,
+                                                        double *cone_count, unsigned long long *accepted,
+                                                        unsigned long long *next_link, unsigned long long *visits,
+                                                        int *err) {
     const unsigned FULL = 0xffffffffu;
     const unsigned lane = threadIdx.x & 31;
-    const uint32_t req = (TYPE == EMPTINESS) ? FLAG_SAMPLENESS : 0u;
-    const uint32_t leaf_flag = (TYPE == EMPTINESS) ? FLAG_EMPTINESS : FLAG_SAMPLENESS;
     const float root_size_f = (float)in.root_size;
-    uint32_t st_node[MAX_TREE_DEPTH];
-    uint8_t st_next[MAX_TREE_DEPTH];
+    // stack of expanded nodes that still have children to descend into
+    uint32_t st_c0[MAX_TREE_DEPTH];
+    uint8_t st_mask[MAX_TREE_DEPTH], st_d[MAX_TREE_DEPTH];
     F3 st_min[MAX_TREE_DEPTH];
     int sp = 0;
-    uint32_t top_node = 0, top_c0 = 0, top_next = 0;
-    F3 top_min = f3(0.f, 0.f, 0.f);
-    uint32_t base = 0, max_depth = 0;
+    // the node to expand next: its children block, box corner and depth
+    bool have = false;
+    uint32_t x_c0 = 0, x_d = 0;
+    F3 x_min = f3(0.f, 0.f, 0.f);
+    uint32_t max_depth = 0;
     ConeF c;
-    float wlen = 0.f, fconf = 0.f;
+    double wlen = 0.0;
+    float fconf = 0.f;
     bool done = false;
     double count = 0.0;
     unsigned long long acc = 0, nvis = 0;
 
-    auto visit_leaf = [&](uint32_t node, F3 bmin, float size) {
+    auto visit_leaf = [&](uint32_t leaf, F3 bmin, float size) {
         float h = 0.5f * size;
         float val;
         if (!eval_kernel(c, bmin + f3(h, h, h), TYPE == SAMPLENESS, fconf, &val)) return;
-        uint32_t leaf = tr.node_to_leaf[node];
-        add_comp(&ksum[leaf], val);
-        add_comp(&clen[leaf], wlen);
-        if ((states[node] & leaf_flag) == 0) atomicOr(&states[node], leaf_flag);
+        atomicAdd(&ksum[leaf], (double)val);
+        atomicAdd(&clen[leaf], wlen);
         ++acc;
     };
 
     while (true) {
-        bool need = (sp == 0) && !done;
+        // resume the deepest expanded node that has children left
+        if (!have && sp > 0) {
+            uint32_t m = st_mask[sp - 1];
+            uint32_t ci = __ffs(m) - 1;
+            uint32_t c0 = st_c0[sp - 1], d = st_d[sp - 1];
+            F3 pmin = st_min[sp - 1];
+            m &= m - 1;
+            if (m) st_mask[sp - 1] = (uint8_t)m; else --sp;
+            float size = ldexpf(root_size_f, -(int)d);
+            x_c0 = __ldg(&rec[c0 + REC_OFFSET + ci]).x;
+            x_min = child_min(pmin, ci, size);
+            x_d = d + 1;
+            have = true;
+        }
+        bool need = !have && !done;
         unsigned nm = __ballot_sync(FULL, need);
         if (nm) {
             int leader = __ffs(nm) - 1;
@@ -370,7 +248,7 @@ __global__ void __launch_bounds__(PT_BLOCK, (TYPE == 0) ? 6 : 5) k_cone_pt(uint6
                     if (!(full > EPS) || !(kernel_r > 0.0) || fabs(denom) <= EPS * full) break;   // isDegenerated
                     double conf = in.conf[s];
                     if (TYPE == EMPTINESS) count += conf;
-                    wlen = (float)(conf * length);
+                    wlen = conf * length;
                     fconf = (float)conf;
                     max_depth = (uint32_t)ceil(log2(in.root_size / (in.scale[s] * in.h_svo))) + MAX_DEPTH_DIFFERENCE;
                     c.apex = f3((float)apex_d.x, (float)apex_d.y, (float)apex_d.z);
@@ -388,11 +266,11 @@ __global__ void __launch_bounds__(PT_BLOCK, (TYPE == 0) ? 6 : 5) k_cone_pt(uint6
                     F3 p0 = c.end + c.axis * c.t_start_e;
                     F3 lo = f3(fminf(p0.x, c.end.x) - c.radius, fminf(p0.y, c.end.y) - c.radius, fminf(p0.z, c.end.z) - c.radius);
                     F3 hi = f3(fmaxf(p0.x, c.end.x) + c.radius, fmaxf(p0.y, c.end.y) + c.radius, fmaxf(p0.z, c.end.z) + c.radius);
-                    uint32_t start = 0;
-                    base = 0;
+                    uint32_t start = 0, base = 0;
+                    uint2 srec = __ldg(&rec[REC_OFFSET]);
                     F3 smin = rel(tr.nmin[0], p);
                     float ssize = root_size_f;
-                    while (tr.children[start] != INVALID && base + 1 <= max_depth) {
+                    while (srec.x != INVALID && base + 1 <= max_depth) {
                         float cs = 0.5f * ssize;
                         float margin = 1e-5f * ssize;
                         F3 ctr = smin + f3(cs, cs, cs);
@@ -405,68 +283,74 @@ __global__ void __launch_bounds__(PT_BLOCK, (TYPE == 0) ? 6 : 5) k_cone_pt(uint6
                             inside = false;
                         }
                         if (!inside) break;
-                        start = tr.children[start] + digit;
+                        start = srec.x + digit;
+                        srec = __ldg(&rec[start + REC_OFFSET]);
                         smin = rel(tr.nmin[start], p);
                         ssize = cs;
                         ++base;
                     }
-                    if (req && (states[start] & req) != req) break;
+                    if (TYPE == EMPTINESS && !(srec.y & REC_FLAG)) break;
                     if (cone_box_separated_pt(c, smin, ssize)) break;
-                    if (tr.children[start] == INVALID) { visit_leaf(start, smin, ssize); break; }
+                    if (srec.x == INVALID) { visit_leaf(srec.y & REC_NOLEAF, smin, ssize); break; }
                     if (base + 1 > max_depth) break;
-                    top_node = start;
-                    top_c0 = tr.children[start];
-                    top_next = 0;
-                    top_min = smin;
-                    sp = 1;
+                    x_c0 = srec.x;
+                    x_min = smin;
+                    x_d = base + 1;
+                    have = true;
                 } while (0);
             }
         }
-        if (__all_sync(FULL, done && sp == 0)) break;
-        if (sp > 0) {
-            // one step of the depth-first traversal (NodesIterator.cpp:38-86);
-            // the top of the stack lives in registers, the rest in local memory
-            if (top_next == 8) {
-                --sp;
-                if (sp > 0) {
-                    top_node = st_node[sp - 1];
-                    top_next = st_next[sp - 1];
-                    top_min = st_min[sp - 1];
-                    top_c0 = tr.children[top_node];
-                }
-            } else {
-                uint32_t ci = top_next++;
-                uint32_t idx = top_c0 + ci;
-                ++nvis;
-                uint32_t d = base + (uint32_t)sp;
-                float size = ldexpf(root_size_f, -(int)d);
-                F3 bmin = f3((ci & 1u) ? top_min.x + size : top_min.x, (ci & 2u) ? top_min.y + size : top_min.y,
-                             (ci & 4u) ? top_min.z + size : top_min.z);
-                uint2 rec = cs[idx];   // (children, state) in one load
-                if (!(req && (rec.y & req) != req)) {
-                    uint32_t cc0 = rec.x;
-                    if (cc0 == INVALID) {
-                        // a leaf: addKernel's exact test decides, no box test needed
-                        visit_leaf(idx, bmin, size);
-                    } else if (d + 1 <= max_depth && !cone_box_separated_pt(c, bmin, size)) {
-                        if (sp >= MAX_TREE_DEPTH) {
-                            atomicExch(err, 1);
-                        } else {
-                            st_node[sp - 1] = top_node;
-                            st_next[sp - 1] = (uint8_t)top_next;
-                            st_min[sp - 1] = top_min;
-                            top_node = idx;
-                            top_c0 = cc0;
-                            top_next = 0;
-                            top_min = bmin;
-                            ++sp;
-                        }
-                    }
-                }
+        if (__all_sync(FULL, done && !have && sp == 0)) break;
+        if (!have) continue;
+        // ---- expand: test the eight children of the node (NodesIterator.cpp:38-86)
+        have = false;
+        if ((x_c0 & 7u) != 1u || x_c0 > 0xFFFFFFF0u) {   // children blocks start at 1 + 8k
+            atomicExch(err, 3);
+            continue;
+        }
+        const uint4 *line = reinterpret_cast<const uint4 *>(rec + x_c0 + REC_OFFSET);
+        uint4 q0 = __ldg(line), q1 = __ldg(line + 1), q2 = __ldg(line + 2), q3 = __ldg(line + 3);
+        const uint32_t rx[8] = {q0.x, q0.z, q1.x, q1.z, q2.x, q2.z, q3.x, q3.z};
+        const uint32_t ry[8] = {q0.y, q0.w, q1.y, q1.w, q2.y, q2.w, q3.y, q3.w};
+        const float size = ldexpf(root_size_f, -(int)x_d);
+        const bool can_descend = x_d + 1 <= max_depth;
+        uint32_t mask = 0;
+        nvis += 8;
+#pragma unroll
+        for (int ci = 0; ci < 8; ++ci) {
+            if (TYPE == EMPTINESS && !(ry[ci] & REC_FLAG)) continue;
+            F3 bmin = child_min(x_min, (uint32_t)ci, size);
+            if (rx[ci] == INVALID) {
+                // a leaf: addKernel's exact test decides, no box test needed
+                visit_leaf(ry[ci] & REC_NOLEAF, bmin, size);
+            } else if (can_descend && !cone_box_separated_pt(c, bmin, size)) {
+                mask |= 1u << ci;
             }
         }
+        if (mask) {
+            uint32_t ci = __ffs(mask) - 1;
+            uint32_t rest = mask & (mask - 1);
+            if (rest) {
+                if (sp >= MAX_TREE_DEPTH) {
+                    atomicExch(err, 1);
+                    continue;
+                }
+                st_c0[sp] = x_c0;
+                st_mask[sp] = (uint8_t)rest;
+                st_d[sp] = (uint8_t)x_d;
+                st_min[sp] = x_min;
+                ++sp;
+            }
+            uint32_t nc = rx[0];
+#pragma unroll
+            for (int k = 1; k < 8; ++k)
+                if (ci == (uint32_t)k) nc = rx[k];
+            x_min = child_min(x_min, ci, size);
+            x_c0 = nc;
+            x_d += 1;
+            have = true;
+        }
     }
-    // warp-level totals (no block barrier: warps finish independently)
     for (int o = 16; o; o >>= 1) {
         count += __shfl_xor_sync(FULL, count, o);
         acc += __shfl_xor_sync(FULL, acc, o);
@@ -479,10 +363,12 @@ __global__ void __launch_bounds__(PT_BLOCK, (TYPE == 0) ? 6 : 5) k_cone_pt(uint6
     }
 }
 
-// (child block, state word) per node, read with one load by the traversals.
-__global__ void k_pack_cs(uint32_t nn, const uint32_t *children, const uint32_t *states, uint2 *out) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < nn) out[i] = make_uint2(children[i], states ? states[i] : 0u);
+// A leaf carries a type's flag exactly when it received a kernel of that type.
+__global__ void k_leaf_flags(uint32_t nl, const uint32_t *leaf_node, const double *ksum, uint32_t *states,
+                             uint32_t flag) {
+    uint32_t l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= nl) return;
+    if (ksum[l] > 0.0) states[leaf_node[l]] |= flag;
 }
 
 __global__ void k_link_cameras(uint64_t nlinks, const uint32_t *links, uint32_t ncams, uint32_t *keys,
@@ -508,8 +394,6 @@ __global__ void k_forward_flag(uint32_t lo, uint32_t hi, const uint32_t *order, 
     states[n] = s;
 }
 
-__device__ inline double comp_value(float2 v) { return (double)v.x + (double)v.y; }
-
 // Cumulative prior sums per node: psum[node * PK + k] = sum of (emptiness,
 // sampleness) cone lengths over SAMPLENESS-flagged leaves of the node's
 // subtree at most k levels below the node.  Built bottom-up, one level per
@@ -517,8 +401,8 @@ __device__ inline double comp_value(float2 v) { return (double)v.x + (double)v.y
 constexpr int PK = 8;
 
 __global__ void k_prior_sums(uint32_t lo, uint32_t hi, const uint32_t *order, const uint32_t *children,
-                             const uint32_t *node_to_leaf, const uint32_t *states, const float2 *elen,
-                             const float2 *slen, double2 *psum) {
+                             const uint32_t *node_to_leaf, const uint32_t *states, const double *elen,
+                             const double *slen, double2 *psum) {
     uint32_t i = lo + blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= hi) return;
     uint32_t n = order[i];
@@ -528,7 +412,7 @@ __global__ void k_prior_sums(uint32_t lo, uint32_t hi, const uint32_t *order, co
         double2 v = make_double2(0.0, 0.0);
         if (states[n] & FLAG_SAMPLENESS) {
             uint32_t l = node_to_leaf[n];
-            v = make_double2(comp_value(elen[l]), comp_value(slen[l]));
+            v = make_double2(elen[l], slen[l]);
         }
         for (int k = 0; k < PK; ++k) dst[k] = v;
         return;
@@ -554,117 +438,172 @@ __device__ inline bool box_inside_sphere(const D3 &mn, double sz, const D3 &c, d
     return dx * dx + dy * dy + dz * dz <= r * r * (1.0 - 1e-9);
 }
 
-// Node record for the prior queries: geometry, child block and the
-// SAMPLENESS flag in one aligned 32-byte sector, so a visit is one load.
-struct __align__(32) PNode {
-    double x, y, z;
-    uint32_t children;
-    uint32_t flagged;
-};
-
-__global__ void k_pack_nodes(uint32_t nn, const uint32_t *children, const D3 *nmin, const uint32_t *states,
-                             PNode *out) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nn) return;
-    D3 m = nmin[i];
-    PNode r;
-    r.x = m.x;
-    r.y = m.y;
-    r.z = m.z;
-    r.children = children[i];
-    r.flagged = states[i] & FLAG_SAMPLENESS;
-    out[i] = r;
-}
-
 // Occupancy::computePriors (Occupancy.cpp:530-568) with a
 // SphereNodeStatesChecker (SphereNodeStatesChecker.cpp:28-36).  The set of
 // summed leaves is the reference's: SAMPLENESS-flagged leaves at most three
 // levels below the query leaf whose box meets the sphere (the exact FP64
 // test); subtrees wholly inside the sphere are added from psum, whose row 0
 // of a leaf is the leaf's own (emptiness, sampleness) cone-length pair.
-__global__ void __launch_bounds__(128) k_priors_h(uint32_t nl, const uint32_t *leaf_node, const D3 *leaf_min,
-                                                  const uint8_t *depth, const PNode *pn, const double2 *psum,
-                                                  double root_size, double rel_radius, double *prior,
-                                                  unsigned long long *visits, int *err) {
-    uint32_t l = blockIdx.x * blockDim.x + threadIdx.x;
-    if (l >= nl) return;
-    uint32_t node = leaf_node[l];
-    uint32_t ld = depth[node];
-    double size = size_at(root_size, ld);
-    D3 mn = leaf_min[l];
-    double half = dmul(0.5, size);
-    D3 center{dadd(mn.x, half), dadd(mn.y, half), dadd(mn.z, half)};
-    double radius = dmul(size, rel_radius);
-    uint32_t max_depth = ld + MAX_DEPTH_DIFFERENCE;
-    double eL = 0.0, sL = 0.0;
+//
+// Run by persistent threads over the traversal records of the cone passes,
+// expanding one node per step: its eight children's records come in one
+// 64-byte line and their FP64 boxes are derived from the parent's corner with
+// the tree build's own recurrence (child_coords, exact), so no node geometry
+// is loaded inside the loop.
+__global__ void __launch_bounds__(PT_BLOCK) k_priors_x(uint32_t nl, const uint32_t *leaf_node, const D3 *leaf_min,
+                                                      const uint8_t *depth, const D3 *nmin, const uint2 *rec,
+                                                      const double2 *psum, double root_size, double rel_radius,
+                                                      double *prior, unsigned long long *next_leaf,
+                                                      unsigned long long *visits, int *err) {
+    const unsigned FULL = 0xffffffffu;
+    const unsigned lane = threadIdx.x & 31;
+    uint32_t st_c0[MAX_TREE_DEPTH];
+    uint8_t st_mask[MAX_TREE_DEPTH], st_d[MAX_TREE_DEPTH];
+    D3 st_min[MAX_TREE_DEPTH];
+    int sp = 0;
+    bool have = false, active = false, done = false;
+    uint32_t x_c0 = 0, x_d = 0;
+    D3 x_min{0.0, 0.0, 0.0};
+    uint32_t l = 0, max_depth = 0;
+    D3 center{0.0, 0.0, 0.0};
+    double radius = 0.0, eL = 0.0, sL = 0.0;
     unsigned long long nvis = 0;
-    // returns 0 = ignored, 1 = add subtree sum, 2 = visit / descend
-    auto classify = [&](const PNode &r, double sz, uint32_t d) -> int {
-        if (!r.flagged) return 0;
-        if (d > max_depth) return 0;
-        D3 bmn{r.x, r.y, r.z};
-        D3 bmx{dadd(bmn.x, sz), dadd(bmn.y, sz), dadd(bmn.z, sz)};
-        if (!aabb_sphere(bmn, bmx, center, radius)) return 0;
-        if (max_depth - d < (uint32_t)PK && box_inside_sphere(bmn, sz, center, radius)) return 1;
-        return 2;
-    };
     auto add_row = [&](uint32_t n, uint32_t k) {
         double2 v = psum[(size_t)n * PK + k];
         eL += v.x;
         sL += v.y;
     };
-    PNode r0 = pn[0];
-    int rc = classify(r0, root_size, 0);
-    if (rc == 1) {
-        add_row(0, max_depth);
-    } else if (rc == 2) {
-        if (r0.children == INVALID) {
-            add_row(0, 0);
-        } else {
-            uint32_t st_c0[MAX_TREE_DEPTH];
-            uint8_t st_next[MAX_TREE_DEPTH];
-            int sp = 1;
-            uint32_t top_c0 = r0.children, top_next = 0;
-            while (sp > 0) {
-                if (top_next == 8) {
-                    --sp;
-                    if (sp > 0) { top_c0 = st_c0[sp - 1]; top_next = st_next[sp - 1]; }
-                    continue;
+    while (true) {
+        if (!have && sp > 0) {
+            uint32_t m = st_mask[sp - 1];
+            uint32_t ci = __ffs(m) - 1;
+            uint32_t c0 = st_c0[sp - 1], d = st_d[sp - 1];
+            D3 pmin = st_min[sp - 1];
+            m &= m - 1;
+            if (m) st_mask[sp - 1] = (uint8_t)m; else --sp;
+            x_c0 = __ldg(&rec[c0 + REC_OFFSET + ci]).x;
+            x_min = child_coords(pmin, ldexp(root_size, -(int)d), ci);
+            x_d = d + 1;
+            have = true;
+        }
+        if (!have && active) {   // query finished
+            prior[l] = eL / (eL + sL);
+            active = false;
+        }
+        bool need = !have && !done;
+        unsigned nm = __ballot_sync(FULL, need);
+        if (nm) {
+            int leader = __ffs(nm) - 1;
+            unsigned long long b = 0;
+            if ((int)lane == leader) b = atomicAdd(next_leaf, (unsigned long long)__popc(nm));
+            b = __shfl_sync(FULL, b, leader);
+            if (need) {
+                uint64_t i = b + __popc(nm & ((1u << lane) - 1u));
+                if (i >= nl) {
+                    done = true;
+                } else {
+                    l = (uint32_t)i;
+                    uint32_t node = leaf_node[l];
+                    uint32_t ld = depth[node];
+                    double size = size_at(root_size, ld);
+                    D3 mn = leaf_min[l];
+                    double half = dmul(0.5, size);
+                    center = D3{dadd(mn.x, half), dadd(mn.y, half), dadd(mn.z, half)};
+                    radius = dmul(size, rel_radius);
+                    max_depth = ld + MAX_DEPTH_DIFFERENCE;
+                    eL = sL = 0.0;
+                    active = true;
+                    // the root (SphereNodeStatesChecker on node 0)
+                    uint2 r0 = __ldg(&rec[REC_OFFSET]);
+                    D3 bmn = nmin[0];
+                    D3 bmx{dadd(bmn.x, root_size), dadd(bmn.y, root_size), dadd(bmn.z, root_size)};
+                    if ((r0.y & REC_FLAG) && aabb_sphere(bmn, bmx, center, radius)) {
+                        if (max_depth < (uint32_t)PK && box_inside_sphere(bmn, root_size, center, radius)) {
+                            add_row(0, max_depth);
+                        } else if (r0.x == INVALID) {
+                            add_row(0, 0);
+                        } else if (1 <= max_depth) {
+                            x_c0 = r0.x;
+                            x_min = bmn;
+                            x_d = 1;
+                            have = true;
+                        }
+                    }
                 }
-                uint32_t idx = top_c0 + top_next++;
-                uint32_t d = (uint32_t)sp;
-                double sz = size_at(root_size, d);
-                ++nvis;
-                PNode r = pn[idx];
-                int c = classify(r, sz, d);
-                if (c == 0) continue;
-                if (c == 1) { add_row(idx, max_depth - d); continue; }
-                if (r.children == INVALID) { add_row(idx, 0); continue; }
-                if (d + 1 > max_depth) continue;
-                if (sp >= MAX_TREE_DEPTH) { atomicExch(err, 2); break; }
-                st_c0[sp - 1] = top_c0;
-                st_next[sp - 1] = (uint8_t)top_next;
-                top_c0 = r.children;
-                top_next = 0;
-                ++sp;
             }
         }
+        if (__all_sync(FULL, done && !have && sp == 0 && !active)) break;
+        if (!have) continue;
+        have = false;
+        if ((x_c0 & 7u) != 1u || x_c0 > 0xFFFFFFF0u) {
+            atomicExch(err, 3);
+            continue;
+        }
+        const uint4 *line = reinterpret_cast<const uint4 *>(rec + x_c0 + REC_OFFSET);
+        uint4 q0 = __ldg(line), q1 = __ldg(line + 1), q2 = __ldg(line + 2), q3 = __ldg(line + 3);
+        const uint32_t rx[8] = {q0.x, q0.z, q1.x, q1.z, q2.x, q2.z, q3.x, q3.z};
+        const uint32_t ry[8] = {q0.y, q0.w, q1.y, q1.w, q2.y, q2.w, q3.y, q3.w};
+        const double cs = ldexp(root_size, -(int)x_d);
+        const uint32_t d = x_d;
+        const bool can_descend = d + 1 <= max_depth;
+        const bool can_add = d <= max_depth && max_depth - d < (uint32_t)PK;
+        uint32_t mask = 0;
+        nvis += 8;
+        if (d <= max_depth) {
+#pragma unroll
+            for (int ci = 0; ci < 8; ++ci) {
+                if (!(ry[ci] & REC_FLAG)) continue;
+                D3 bmn = child_coords(x_min, cs, (uint32_t)ci);
+                D3 bmx{dadd(bmn.x, cs), dadd(bmn.y, cs), dadd(bmn.z, cs)};
+                if (!aabb_sphere(bmn, bmx, center, radius)) continue;
+                if (can_add && box_inside_sphere(bmn, cs, center, radius)) {
+                    add_row(x_c0 + ci, max_depth - d);
+                } else if (rx[ci] == INVALID) {
+                    add_row(x_c0 + ci, 0);
+                } else if (can_descend) {
+                    mask |= 1u << ci;
+                }
+            }
+        }
+        if (mask) {
+            uint32_t ci = __ffs(mask) - 1;
+            uint32_t rest = mask & (mask - 1);
+            if (rest) {
+                if (sp >= MAX_TREE_DEPTH) {
+                    atomicExch(err, 2);
+                    continue;
+                }
+                st_c0[sp] = x_c0;
+                st_mask[sp] = (uint8_t)rest;
+                st_d[sp] = (uint8_t)d;
+                st_min[sp] = x_min;
+                ++sp;
+            }
+            uint32_t nc = rx[0];
+#pragma unroll
+            for (int k = 1; k < 8; ++k)
+                if (ci == (uint32_t)k) nc = rx[k];
+            x_min = child_coords(x_min, cs, ci);
+            x_c0 = nc;
+            x_d = d + 1;
+            have = true;
+        }
     }
-    prior[l] = eL / (eL + sL);
-    if (nvis) atomicAdd(visits, nvis);
+    for (int o = 16; o; o >>= 1) nvis += __shfl_xor_sync(FULL, nvis, o);
+    if (lane == 0 && nvis) atomicAdd(visits, nvis);
 }
 
 // Occupancy::getOccupancy (Occupancy.cpp:570-587), FP64.
-__global__ void k_finalize(uint32_t nl, const float2 *esum, const float2 *ssum, const float2 *elen,
-                           const float2 *slen, const double *prior, double cone_count, double threshold,
+__global__ void k_finalize(uint32_t nl, const double *esum, const double *ssum, const double *elen,
+                           const double *slen, const double *prior, double cone_count, double threshold,
                            double *o_esum, double *o_ssum, double *o_elen, double *o_slen, double *occ) {
     uint32_t l = blockIdx.x * blockDim.x + threadIdx.x;
     if (l >= nl) return;
-    double e = comp_value(esum[l]), s = comp_value(ssum[l]);
+    double e = esum[l], s = ssum[l];
     o_esum[l] = e;
     o_ssum[l] = s;
-    o_elen[l] = comp_value(elen[l]);
-    o_slen[l] = comp_value(slen[l]);
+    o_elen[l] = elen[l];
+    o_slen[l] = slen[l];
     double v;
     if ((e + s) < threshold) {
         v = -EPS;
@@ -708,9 +647,9 @@ void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_
     Timer timer(st);
     DBuf<D3> cams(cv.count, st);
     if (cv.count) TSR_CUDA(cudaMemcpyAsync(cams.p, cv.positions, (size_t)cv.count * 24, cudaMemcpyHostToDevice, st));
-    DBuf<float2> acc(4ull * nl, st);   // esum, ssum, elen, slen
+    DBuf<double> acc(4ull * nl, st);   // esum, ssum, elen, slen
     acc.zero();
-    float2 *esum = acc.p, *ssum = acc.p + nl, *elen = acc.p + 2ull * nl, *slen = acc.p + 3ull * nl;
+    double *esum = acc.p, *ssum = acc.p + nl, *elen = acc.p + 2ull * nl, *slen = acc.p + 3ull * nl;
     o.states.alloc(nn, st);
     o.states.zero();
     DBuf<double> cone_count(1, st);
@@ -722,36 +661,29 @@ void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_
 
     LinkIn in{t.pos.p, t.nrm.p, t.scale.p, t.conf.p, t.links.p, cams.p, t.k, cv.count,
               p.max_relative_sampling_distance, p.bandwidth_factor, p.relative_sample_cone_length, t.root_size};
-    TreeIn tr{t.children.p, t.depth.p, t.nmin.p, t.node_to_leaf.p};
+    TreeIn tr{t.nmin.p};
     uint64_t nlinks = (uint64_t)t.n_samples * t.k;
     o.links = nlinks;
-    unsigned grid = (unsigned)((nlinks + 127) / 128);
-    if (grid == 0) grid = 1;
     DBuf<unsigned long long> next_link(1, st);
-    unsigned pt_grid = 0;
+    unsigned x_grid = 0, prior_grid = 0;
     {
         int dev = 0, sms = 0, per_sm = 0;
         TSR_CUDA(cudaGetDevice(&dev));
         TSR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        TSR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cone_pt<EMPTINESS>, PT_BLOCK, 0));
-        pt_grid = (unsigned)(sms * (per_sm > 0 ? per_sm : 1));
+        TSR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cone_x<EMPTINESS>, PT_BLOCK, 0));
+        x_grid = (unsigned)(sms * (per_sm > 0 ? per_sm : 1));
+        TSR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_priors_x, PT_BLOCK, 0));
+        prior_grid = (unsigned)(sms * (per_sm > 0 ? per_sm : 1));
     }
-    // TSR_CONE_KERNEL=thread selects the one-thread-per-link kernel (same
-    // traversal and results, no persistent scheduling) for comparisons
-    const char *kenv = getenv("TSR_CONE_KERNEL");
-    const bool per_thread = kenv && kenv[0] == 't';
-    DBuf<uint2> packed(nn, st);
-    k_pack_cs<<<grid_for(nn, BLK), BLK, 0, st>>>(nn, t.children.p, nullptr, packed.p); ::tsr::note_launch();
-    if (per_thread) {
-        k_cone_pass<SAMPLENESS><<<grid, 128, 0, st>>>(nlinks, in, tr, o.states.p, ssum, slen, cone_count.p,
-                                                      accepted.p + 1, err.p);
-    } else {
-        next_link.zero();
-        k_cone_pt<SAMPLENESS><<<pt_grid, PT_BLOCK, 0, st>>>(nlinks, nullptr, in, tr, packed.p, o.states.p, ssum, slen,
-                                                           cone_count.p, accepted.p + 1, next_link.p,
-                                                           accepted.p + 3, err.p);
-    }
+    if (nl > REC_NOLEAF) fail(TSR_ERR_OVERFLOW_U32, "leaf count must stay below 2^31 - 1 for the traversal records");
+    DBuf<uint2> recs((size_t)nn + 8, st);
+    if (reinterpret_cast<uintptr_t>(recs.p) % 16) fail(TSR_ERR_CUDA, "traversal records are not 16-byte aligned");
+    next_link.zero();
+    k_pack_rec<<<grid_for(nn, BLK), BLK, 0, st>>>(nn, t.children.p, t.node_to_leaf.p, nullptr, recs.p); ::tsr::note_launch();
+    k_cone_x<SAMPLENESS><<<x_grid, PT_BLOCK, 0, st>>>(nlinks, nullptr, in, tr, recs.p, ssum, slen, cone_count.p,
+                                                     accepted.p + 1, next_link.p, accepted.p + 3, err.p);
     ::tsr::note_launch();
+    k_leaf_flags<<<grid_for(nl, BLK), BLK, 0, st>>>(nl, t.leaf_node.p, ssum, o.states.p, FLAG_SAMPLENESS); ::tsr::note_launch();
     o.stage_ms[0] = timer.lap();
     // EMPTINESS links grouped by camera (stable, so sample order is kept
     // within a camera): a warp's cones then share their apex
@@ -772,18 +704,13 @@ void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_
         k_forward_flag<<<grid_for(hi - lo, BLK), BLK, 0, st>>>(lo, hi, t.level_order.p, t.children.p, o.states.p,
                                                               FLAG_SAMPLENESS); ::tsr::note_launch();
     }
-    k_pack_cs<<<grid_for(nn, BLK), BLK, 0, st>>>(nn, t.children.p, o.states.p, packed.p); ::tsr::note_launch();
+    k_pack_rec<<<grid_for(nn, BLK), BLK, 0, st>>>(nn, t.children.p, t.node_to_leaf.p, o.states.p, recs.p); ::tsr::note_launch();
     o.stage_ms[1] = timer.lap();
-    if (per_thread) {
-        k_cone_pass<EMPTINESS><<<grid, 128, 0, st>>>(nlinks, in, tr, o.states.p, esum, elen, cone_count.p, accepted.p,
-                                                     err.p);
-    } else {
-        next_link.zero();
-        k_cone_pt<EMPTINESS><<<pt_grid, PT_BLOCK, 0, st>>>(nlinks, order.p, in, tr, packed.p, o.states.p, esum, elen,
-                                                          cone_count.p, accepted.p, next_link.p, accepted.p + 2,
-                                                          err.p);
-    }
+    next_link.zero();
+    k_cone_x<EMPTINESS><<<x_grid, PT_BLOCK, 0, st>>>(nlinks, order.p, in, tr, recs.p, esum, elen, cone_count.p,
+                                                    accepted.p, next_link.p, accepted.p + 2, err.p);
     ::tsr::note_launch();
+    k_leaf_flags<<<grid_for(nl, BLK), BLK, 0, st>>>(nl, t.leaf_node.p, esum, o.states.p, FLAG_EMPTINESS); ::tsr::note_launch();
     o.stage_ms[2] = timer.lap();
     o.prior.alloc(nl, st);
     {
@@ -793,11 +720,10 @@ void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_
             k_prior_sums<<<grid_for(hi - lo, BLK), BLK, 0, st>>>(lo, hi, t.level_order.p, t.children.p,
                                                                 t.node_to_leaf.p, o.states.p, elen, slen, psum.p); ::tsr::note_launch();
         }
-        DBuf<PNode> pn(nn, st);
-        k_pack_nodes<<<grid_for(nn, BLK), BLK, 0, st>>>(nn, t.children.p, t.nmin.p, o.states.p, pn.p); ::tsr::note_launch();
-        k_priors_h<<<grid_for(nl, 128), 128, 0, st>>>(nl, t.leaf_node.p, t.leaf_min.p, t.depth.p, pn.p, psum.p,
-                                                     t.root_size, p.relative_radius_for_priors, o.prior.p,
-                                                     accepted.p + 4, err.p);
+        next_link.zero();
+        k_priors_x<<<prior_grid, PT_BLOCK, 0, st>>>(nl, t.leaf_node.p, t.leaf_min.p, t.depth.p, t.nmin.p, recs.p,
+                                                   psum.p, t.root_size, p.relative_radius_for_priors, o.prior.p,
+                                                   next_link.p, accepted.p + 4, err.p);
         ::tsr::note_launch();
     }
     o.stage_ms[3] = timer.lap();
@@ -815,6 +741,7 @@ void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_
     o.visits[0] = a[2];
     o.visits[1] = a[3];
     o.visits[2] = a[4];
+    if (e == 3) fail(TSR_ERR_DEVICE_ASSERT, "occupancy traversal met a children block off its 8-node alignment");
     if (e) fail(TSR_ERR_DEVICE_ASSERT, "occupancy traversal exceeded its stack bound");
     TSR_CUDA(cudaGetLastError());
 }
