@@ -308,7 +308,7 @@ def our_arm(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
         "config": {"workload": desc, "samples": n, "cameras": int(scene.cams.shape[0]), "k": K,
-                   "mode": "plain FP32 field (compensated sums), FP64 topology",
+                   "mode": "plain path: FP32 kernel evaluation with FP64 per-leaf accumulation, FP64 topology",
                    "l2": "inputs %d MB > 126 MB L2; all buffers re-allocated each step" % (h2d // 2**20),
                    "parallelism": "replicas" if world > 1 else "single GPU",
                    "nodes": Nn, "leaves": Nl, "dual_cells": tc.dual_cells, "triangles": mc.triangles,

@@ -169,10 +169,9 @@ __global__ void __launch_bounds__(PT_BLOCK, (TYPE == 0) ? 6 : 5) k_cone_x(uint64
     const unsigned lane = threadIdx.x & 31;
     const float root_size_f = (float)in.root_size;
     // stack of expanded nodes that still have children to descend into
-    uint32_t st_c0[MAX_TREE_DEPTH];
-    uint8_t st_mask[MAX_TREE_DEPTH], st_d[MAX_TREE_DEPTH];
-    F3 st_min[MAX_TREE_DEPTH];
+    uint64_t st[MAX_TREE_DEPTH];   // children block | mask << 32 | depth << 40
     int sp = 0;
+    D3 spos{0.0, 0.0, 0.0};        // the link's sample: origin of the FP32 frame
     // the node to expand next: its children block, box corner and depth
     bool have = false;
     uint32_t x_c0 = 0, x_d = 0;
@@ -197,16 +196,14 @@ __global__ void __launch_bounds__(PT_BLOCK, (TYPE == 0) ? 6 : 5) k_cone_x(uint64
     while (true) {
         // resume the deepest expanded node that has children left
         if (!have && sp > 0) {
-            uint32_t m = st_mask[sp - 1];
-            uint32_t ci = __ffs(m) - 1;
-            uint32_t c0 = st_c0[sp - 1], d = st_d[sp - 1];
-            F3 pmin = st_min[sp - 1];
+            uint64_t e = st[sp - 1];
+            uint32_t m = (uint32_t)(e >> 32) & 0xFFu;
+            uint32_t node = (uint32_t)e + (uint32_t)(__ffs(m) - 1);
             m &= m - 1;
-            if (m) st_mask[sp - 1] = (uint8_t)m; else --sp;
-            float size = ldexpf(root_size_f, -(int)d);
-            x_c0 = __ldg(&rec[c0 + REC_OFFSET + ci]).x;
-            x_min = child_min(pmin, ci, size);
-            x_d = d + 1;
+            if (m) st[sp - 1] = (e & ~(0xFFull << 32)) | ((uint64_t)m << 32); else --sp;
+            x_c0 = __ldg(&rec[node + REC_OFFSET]).x;
+            x_min = rel(tr.nmin[node], spos);
+            x_d = (uint32_t)(e >> 40) + 1;
             have = true;
         }
         bool need = !have && !done;
@@ -227,6 +224,7 @@ __global__ void __launch_bounds__(PT_BLOCK, (TYPE == 0) ? 6 : 5) k_cone_x(uint64
                     uint32_t cam = in.links[l];
                     if (cam == INVALID || cam >= in.ncams) break;
                     D3 p = in.pos[s];
+                    spos = p;
                     D3 n = in.nrm[s];
                     D3 cwp = in.cams[cam];
                     double kernel_r = in.h_o * in.scale[s];
@@ -335,11 +333,7 @@ __global__ void __launch_bounds__(PT_BLOCK, (TYPE == 0) ? 6 : 5) k_cone_x(uint64
                     atomicExch(err, 1);
                     continue;
                 }
-                st_c0[sp] = x_c0;
-                st_mask[sp] = (uint8_t)rest;
-                st_d[sp] = (uint8_t)x_d;
-                st_min[sp] = x_min;
-                ++sp;
+                st[sp++] = (uint64_t)x_c0 | ((uint64_t)rest << 32) | ((uint64_t)x_d << 40);
             }
             uint32_t nc = rx[0];
 #pragma unroll
@@ -394,38 +388,39 @@ __global__ void k_forward_flag(uint32_t lo, uint32_t hi, const uint32_t *order, 
     states[n] = s;
 }
 
-// Cumulative prior sums per node: psum[node * PK + k] = sum of (emptiness,
+// Cumulative prior sums per node: psum[k * nn + node] = sum of (emptiness,
 // sampleness) cone lengths over SAMPLENESS-flagged leaves of the node's
 // subtree at most k levels below the node.  Built bottom-up, one level per
-// launch.
+// launch.  Rows are k-major so that the eight siblings of a children block
+// share one 128-byte line per k.
 constexpr int PK = 8;
 
-__global__ void k_prior_sums(uint32_t lo, uint32_t hi, const uint32_t *order, const uint32_t *children,
-                             const uint32_t *node_to_leaf, const uint32_t *states, const double *elen,
-                             const double *slen, double2 *psum) {
+__global__ void k_prior_sums(uint32_t lo, uint32_t hi, uint32_t nn, const uint32_t *order,
+                             const uint32_t *children, const uint32_t *node_to_leaf, const uint32_t *states,
+                             const double *elen, const double *slen, double2 *psum) {
     uint32_t i = lo + blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= hi) return;
     uint32_t n = order[i];
     uint32_t c0 = children[n];
-    double2 *dst = psum + (size_t)n * PK;
     if (c0 == INVALID) {
         double2 v = make_double2(0.0, 0.0);
         if (states[n] & FLAG_SAMPLENESS) {
             uint32_t l = node_to_leaf[n];
             v = make_double2(elen[l], slen[l]);
         }
-        for (int k = 0; k < PK; ++k) dst[k] = v;
+        for (int k = 0; k < PK; ++k) psum[(size_t)k * nn + n] = v;
         return;
     }
-    dst[0] = make_double2(0.0, 0.0);
+    psum[n] = make_double2(0.0, 0.0);
     for (int k = 1; k < PK; ++k) {
+        const double2 *row = psum + (size_t)(k - 1) * nn + c0;
         double e = 0.0, s = 0.0;
         for (uint32_t c = 0; c < 8; ++c) {
-            double2 v = psum[(size_t)(c0 + c) * PK + k - 1];
+            double2 v = row[c];
             e += v.x;
             s += v.y;
         }
-        dst[k] = make_double2(e, s);
+        psum[(size_t)k * nn + n] = make_double2(e, s);
     }
 }
 
@@ -450,16 +445,14 @@ __device__ inline bool box_inside_sphere(const D3 &mn, double sz, const D3 &c, d
 // 64-byte line and their FP64 boxes are derived from the parent's corner with
 // the tree build's own recurrence (child_coords, exact), so no node geometry
 // is loaded inside the loop.
-__global__ void __launch_bounds__(PT_BLOCK) k_priors_x(uint32_t nl, const uint32_t *leaf_node, const D3 *leaf_min,
+__global__ void __launch_bounds__(PT_BLOCK) k_priors_x(uint32_t nl, uint32_t nn, const uint32_t *leaf_node, const D3 *leaf_min,
                                                       const uint8_t *depth, const D3 *nmin, const uint2 *rec,
                                                       const double2 *psum, double root_size, double rel_radius,
                                                       double *prior, unsigned long long *next_leaf,
                                                       unsigned long long *visits, int *err) {
     const unsigned FULL = 0xffffffffu;
     const unsigned lane = threadIdx.x & 31;
-    uint32_t st_c0[MAX_TREE_DEPTH];
-    uint8_t st_mask[MAX_TREE_DEPTH], st_d[MAX_TREE_DEPTH];
-    D3 st_min[MAX_TREE_DEPTH];
+    uint64_t st[MAX_TREE_DEPTH];   // children block | mask << 32 | depth << 40
     int sp = 0;
     bool have = false, active = false, done = false;
     uint32_t x_c0 = 0, x_d = 0;
@@ -469,21 +462,20 @@ __global__ void __launch_bounds__(PT_BLOCK) k_priors_x(uint32_t nl, const uint32
     double radius = 0.0, eL = 0.0, sL = 0.0;
     unsigned long long nvis = 0;
     auto add_row = [&](uint32_t n, uint32_t k) {
-        double2 v = psum[(size_t)n * PK + k];
+        double2 v = psum[(size_t)k * nn + n];
         eL += v.x;
         sL += v.y;
     };
     while (true) {
         if (!have && sp > 0) {
-            uint32_t m = st_mask[sp - 1];
-            uint32_t ci = __ffs(m) - 1;
-            uint32_t c0 = st_c0[sp - 1], d = st_d[sp - 1];
-            D3 pmin = st_min[sp - 1];
+            uint64_t e = st[sp - 1];
+            uint32_t m = (uint32_t)(e >> 32) & 0xFFu;
+            uint32_t node = (uint32_t)e + (uint32_t)(__ffs(m) - 1);
             m &= m - 1;
-            if (m) st_mask[sp - 1] = (uint8_t)m; else --sp;
-            x_c0 = __ldg(&rec[c0 + REC_OFFSET + ci]).x;
-            x_min = child_coords(pmin, ldexp(root_size, -(int)d), ci);
-            x_d = d + 1;
+            if (m) st[sp - 1] = (e & ~(0xFFull << 32)) | ((uint64_t)m << 32); else --sp;
+            x_c0 = __ldg(&rec[node + REC_OFFSET]).x;
+            x_min = nmin[node];   // the build's own FP64 corner of that node
+            x_d = (uint32_t)(e >> 40) + 1;
             have = true;
         }
         if (!have && active) {   // query finished
@@ -573,11 +565,7 @@ __global__ void __launch_bounds__(PT_BLOCK) k_priors_x(uint32_t nl, const uint32
                     atomicExch(err, 2);
                     continue;
                 }
-                st_c0[sp] = x_c0;
-                st_mask[sp] = (uint8_t)rest;
-                st_d[sp] = (uint8_t)d;
-                st_min[sp] = x_min;
-                ++sp;
+                st[sp++] = (uint64_t)x_c0 | ((uint64_t)rest << 32) | ((uint64_t)d << 40);
             }
             uint32_t nc = rx[0];
 #pragma unroll
@@ -717,11 +705,11 @@ void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_
         DBuf<double2> psum((size_t)nn * PK, st);
         for (int d = (int)t.level_start.size() - 2; d >= 0; --d) {
             uint32_t lo = t.level_start[d], hi = t.level_start[d + 1];
-            k_prior_sums<<<grid_for(hi - lo, BLK), BLK, 0, st>>>(lo, hi, t.level_order.p, t.children.p,
+            k_prior_sums<<<grid_for(hi - lo, BLK), BLK, 0, st>>>(lo, hi, nn, t.level_order.p, t.children.p,
                                                                 t.node_to_leaf.p, o.states.p, elen, slen, psum.p); ::tsr::note_launch();
         }
         next_link.zero();
-        k_priors_x<<<prior_grid, PT_BLOCK, 0, st>>>(nl, t.leaf_node.p, t.leaf_min.p, t.depth.p, t.nmin.p, recs.p,
+        k_priors_x<<<prior_grid, PT_BLOCK, 0, st>>>(nl, nn, t.leaf_node.p, t.leaf_min.p, t.depth.p, t.nmin.p, recs.p,
                                                    psum.p, t.root_size, p.relative_radius_for_priors, o.prior.p,
                                                    next_link.p, accepted.p + 4, err.p);
         ::tsr::note_launch();
