@@ -60,17 +60,14 @@ struct TreeIn {
 };
 
 
-// Occupancy::addKernel (Occupancy.cpp:279-346) at leaf centre x.
-__device__ inline bool eval_kernel(const ConeF &c, F3 x, bool sampleness, float conf, float *out) {
-    F3 u = x - c.end;
-    float te = fdot(u, c.m) * c.inv_denom;        // tComplete - 1
+// Occupancy::addKernel (Occupancy.cpp:279-346) at a leaf centre x, given
+// te = dot(x - end, m) / denom (= tComplete - 1) and r2 = |x - PCD centre|^2.
+__device__ inline bool kernel_at(const ConeF &c, float te, float r2, bool sampleness, float conf, float *out) {
     float tcut_m1 = te * c.a_over_l;               // tCut - 1
     float tcut = 1.0f + tcut_m1;
     if (tcut < 0.0f || tcut >= 1.0f) return false;
     float tc = 1.0f + te;
-    F3 q = u - c.axis * te;                        // x - PCD centre
     float pr = c.radius * tc;
-    float r2 = fdot(q, q);
     float pr2 = pr * pr;
     if (r2 >= pr2) return false;
     float ray;
@@ -91,6 +88,20 @@ __device__ inline bool eval_kernel(const ConeF &c, F3 x, bool sampleness, float 
     if (!(scaled >= (float)EPS)) return false;
     *out = scaled;
     return true;
+}
+
+// Cone-frame coordinates of point x: te and the squared distance to the axis.
+__device__ __forceinline__ void cone_coords(const ConeF &c, F3 x, float &te, float &r2) {
+    F3 u = x - c.end;
+    te = fdot(u, c.m) * c.inv_denom;
+    F3 q = u - c.axis * te;
+    r2 = fdot(q, q);
+}
+
+__device__ inline bool eval_kernel(const ConeF &c, F3 x, bool sampleness, float conf, float *out) {
+    float te, r2;
+    cone_coords(c, x, te, r2);
+    return kernel_at(c, te, r2, sampleness, conf, out);
 }
 
 __device__ inline F3 rel(const D3 &a, const D3 &origin) {
@@ -116,6 +127,19 @@ __device__ inline bool cone_box_separated_pt(const ConeF &c, F3 bmin, float size
     if (1.0f + te + dt <= 0.0f) return true;
     F3 q = u - c.axis * te;
     float qn = sqrtf(fdot(q, q));
+    float tmax = fminf(1.0f + te + dt, 1.0f);
+    float bound = qn - hs * 1.7320508f - dt * c.full;
+    return bound > tmax * c.radius * 1.0001f + 1e-4f * (qn + hs + dt * c.full);
+}
+
+// The same test for a box of centre coordinates (te, r2) and half size hs
+// already widened by the recurrence slack; dt = hs * |m|_1 * |1/denom|.
+__device__ __forceinline__ bool separated_at(const ConeF &c, float te, float r2, float hs, float dt) {
+    float slack = 1e-4f * (dt + fabsf(te)) + 1e-6f;
+    if (te + dt < c.t_start_e - slack) return true;
+    if (te - dt >= slack) return true;
+    if (1.0f + te + dt <= 0.0f) return true;
+    float qn = sqrtf(r2);
     float tmax = fminf(1.0f + te + dt, 1.0f);
     float bound = qn - hs * 1.7320508f - dt * c.full;
     return bound > tmax * c.radius * 1.0001f + 1e-4f * (qn + hs + dt * c.full);
@@ -312,16 +336,31 @@ __global__ void __launch_bounds__(PT_BLOCK, (TYPE == 0) ? 6 : 5) k_cone_x(uint64
         const uint32_t ry[8] = {q0.y, q0.w, q1.y, q1.w, q2.y, q2.w, q3.y, q3.w};
         const float size = ldexpf(root_size_f, -(int)x_d);
         const bool can_descend = x_d + 1 <= max_depth;
+        // one widened half size for all eight boxes: covers the FP32 corner
+        // error of every child centre (|centre|_1 <= |x_min|_1 + 4.5 size)
+        const float h = 0.5f * size;
+        const float hs = h + 2e-6f * (fabsf(x_min.x) + fabsf(x_min.y) + fabsf(x_min.z) + 4.5f * size);
+        const float dt = hs * c.n1 * fabsf(c.inv_denom);
+        const F3 ctr0 = x_min + f3(h, h, h);
         uint32_t mask = 0;
         nvis += 8;
 #pragma unroll
         for (int ci = 0; ci < 8; ++ci) {
             if (TYPE == EMPTINESS && !(ry[ci] & REC_FLAG)) continue;
-            F3 bmin = child_min(x_min, (uint32_t)ci, size);
+            F3 ctr = f3((ci & 1) ? ctr0.x + size : ctr0.x, (ci & 2) ? ctr0.y + size : ctr0.y,
+                        (ci & 4) ? ctr0.z + size : ctr0.z);
+            float te, r2;
+            cone_coords(c, ctr, te, r2);
             if (rx[ci] == INVALID) {
                 // a leaf: addKernel's exact test decides, no box test needed
-                visit_leaf(ry[ci] & REC_NOLEAF, bmin, size);
-            } else if (can_descend && !cone_box_separated_pt(c, bmin, size)) {
+                float val;
+                if (kernel_at(c, te, r2, TYPE == SAMPLENESS, fconf, &val)) {
+                    uint32_t leaf = ry[ci] & REC_NOLEAF;
+                    atomicAdd(&ksum[leaf], (double)val);
+                    atomicAdd(&clen[leaf], wlen);
+                    ++acc;
+                }
+            } else if (can_descend && !separated_at(c, te, r2, hs, dt)) {
                 mask |= 1u << ci;
             }
         }

@@ -207,44 +207,96 @@ __device__ inline bool leaf_reliable(const D3 &mn, double size, const SampleRef 
     return false;
 }
 
-// Nodes::findReliableSamplingNode (Nodes.cpp:433-469) from the root over the
-// versioned tree; calls on_read(leaf) for every leaf it rejects.  Returns
-// the reliable leaf or INVALID.
+// Deepest node of the versioned tree whose box contains the side's sphere
+// (radius r around the sample) with a margin: every node outside its subtree
+// is then disjoint from the sphere by at least the margin, so the exact tests
+// of the reference reject all of them, and the descent's best child along
+// the path is always the one containing the sphere.  Both searches can start
+// there and give the reference's results.  The margin, 1e-12 of the largest
+// coordinate magnitude plus the root size, dwarfs the FP64 rounding of the
+// corner recurrence and of the tests.
+__device__ inline uint32_t sphere_start_v(const NV &v, const Root &root, uint32_t key, const SampleRef &q,
+                                          double margin) {
+    uint32_t node = 0;
+    D3 mn = root.mn;
+    uint32_t d = 0;
+    const double lo[3] = {q.p.x - q.r, q.p.y - q.r, q.p.z - q.r};
+    const double hi[3] = {q.p.x + q.r, q.p.y + q.r, q.p.z + q.r};
+    while (!leaf_v(v, node, key) && d < MAX_TREE_DEPTH) {
+        double cs = size_at(root.size, d + 1);
+        const double c3[3] = {dadd(mn.x, cs), dadd(mn.y, cs), dadd(mn.z, cs)};
+        uint32_t digit = 0;
+        for (int a = 0; a < 3; ++a) {
+            if (hi[a] < c3[a] - margin) continue;
+            if (lo[a] > c3[a] + margin) { digit |= 1u << a; continue; }
+            return node;
+        }
+        node = v.children[node] + digit;
+        mn = child_coords(mn, cs, digit);
+        ++d;
+    }
+    return node;
+}
+
+// Nodes::findReliableSamplingNode (Nodes.cpp:433-469) over the versioned
+// tree, from `start` (the root, or a node that contains the side's sphere,
+// see sphere_start_v); calls on_read(leaf) for every leaf it rejects.
+// Returns the reliable leaf or INVALID.  The order is the reference's
+// depth-first order (children 0..7, each subtree before the next sibling),
+// which decides the returned leaf.
 template <class OnRead>
-__device__ uint32_t find_reliable_v(const NV &v, const Root &root, uint32_t key, const SampleRef &q,
-                                    OnRead on_read, int *err) {
-    if (leaf_v(v, 0, key)) {
-        if (leaf_reliable(root.mn, root.size, q)) return 0;
-        on_read(0u);
+__device__ uint32_t find_reliable_v(const NV &v, const Root &root, uint32_t start, uint32_t key,
+                                    const SampleRef &q, OnRead on_read, int *err) {
+    if (leaf_v(v, start, key)) {
+        D3 smn = start ? v.nmin[start] : root.mn;
+        double ssz = start ? size_at(root.size, v.depth[start]) : root.size;
+        if (leaf_reliable(smn, ssz, q)) return start;
+        on_read(start);
         return INVALID;
     }
-    uint32_t st_node[MAX_TREE_DEPTH];
-    uint8_t st_next[MAX_TREE_DEPTH];
+    // The node being scanned lives in registers (its children block, corner,
+    // depth and next child); children's corners come from the build's own
+    // recurrence (child_coords, exact), so a child costs a load only when it
+    // meets the side.  Stack entries are (node, next child); resuming reloads
+    // the node's block, corner and depth.
+    uint64_t st[MAX_TREE_DEPTH];
     int sp = 0;
-    st_node[0] = 0;
-    st_next[0] = 0;
-    sp = 1;
-    while (sp > 0) {
-        int t = sp - 1;
-        if (st_next[t] == 8) { --sp; continue; }
-        uint32_t c = st_next[t]++;
-        uint32_t parent = st_node[t];
-        uint32_t idx = v.children[parent] + c;
-        uint32_t d = v.depth[idx];
-        double cs = size_at(root.size, d);
-        D3 cmn = v.nmin[idx];
+    uint32_t cur = start, c0 = v.children[start], next = 0, d = v.depth[start];
+    D3 pmn = start ? v.nmin[start] : root.mn;
+    double cs = size_at(root.size, d + 1);
+    while (true) {
+        if (next == 8) {
+            if (sp == 0) return INVALID;
+            uint64_t e = st[--sp];
+            cur = (uint32_t)e;
+            next = (uint32_t)(e >> 32);
+            c0 = v.children[cur];
+            d = v.depth[cur];
+            pmn = cur ? v.nmin[cur] : root.mn;
+            cs = size_at(root.size, d + 1);
+            continue;
+        }
+        uint32_t c = next++;
+        D3 cmn = child_coords(pmn, cs, c);
         if (!intersect_side(cmn, cs, q)) continue;
-        if (leaf_v(v, idx, key)) {
+        uint32_t idx = c0 + c;
+        uint32_t ch = v.children[idx];
+        if (ch == INVALID || v.cc[idx] >= key) {   // leaf_v
             if (leaf_reliable(cmn, cs, q)) return idx;
             on_read(idx);
             continue;
         }
-        if (sp >= MAX_TREE_DEPTH) { *err = 1; return INVALID; }
-        st_node[sp] = idx;
-        st_next[sp] = 0;
-        ++sp;
+        if (next < 8) {   // nothing to resume after the last child
+            if (sp >= MAX_TREE_DEPTH) { *err = 1; return INVALID; }
+            st[sp++] = (uint64_t)cur | ((uint64_t)next << 32);
+        }
+        cur = idx;
+        c0 = ch;
+        pmn = cmn;
+        ++d;
+        cs = dmul(cs, 0.5);
+        next = 0;
     }
-    return INVALID;
 }
 
 // Child with the largest overlap with the sampling segment (Nodes.cpp:300-331).
@@ -271,10 +323,12 @@ __device__ inline D3 segment_end(const SampleRef &q) {
     return D3{dadd(q.p.x, dmul(q.n.x, r)), dadd(q.p.y, dmul(q.n.y, r)), dadd(q.p.z, dmul(q.n.z, r))};
 }
 
-// Leaf the best-overlap descent from the root reaches in the versioned tree.
-__device__ inline uint32_t descent_leaf_v(const NV &v, const Root &root, uint32_t key, const SampleRef &q, int *err) {
+// Leaf the best-overlap descent from the root reaches in the versioned tree
+// (started at a node that contains the side's sphere, see sphere_start_v).
+__device__ inline uint32_t descent_leaf_v(const NV &v, const Root &root, uint32_t start, uint32_t key,
+                                          const SampleRef &q, int *err) {
     D3 endp = segment_end(q);
-    uint32_t node = 0;
+    uint32_t node = start;
     for (int guard = 0; guard < 4 * MAX_TREE_DEPTH; ++guard) {
         if (leaf_v(v, node, key)) return node;
         double sz = size_at(root.size, v.depth[node]);
@@ -286,19 +340,24 @@ __device__ inline uint32_t descent_leaf_v(const NV &v, const Root &root, uint32_
     return node;
 }
 
-// Round evaluation: status 1 = reliable (witness), 2 = writer.
+// Round evaluation: status 1 = reliable (witness), 2 = writer.  Also counts
+// each side's dependency pairs (1 for a witness; the rejected leaves plus the
+// descent leaf for a writer).
 __global__ void k_sampling_eval(uint32_t m, const uint32_t *keys, NV v, Root root, const D3 *pos, const D3 *nrm,
                                 const double *scale, double h_svo, uint8_t *status, uint32_t *witness,
-                                uint32_t *dleaf, int *err) {
+                                uint32_t *dleaf, uint32_t *cnt, double margin, int *err) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m) return;
     uint32_t key = keys[i];
     SampleRef q = sample_side(key, pos, nrm, scale, h_svo);
     int e = 0;
-    uint32_t w = find_reliable_v(v, root, key, q, [](uint32_t) {}, &e);
+    uint32_t reads = 0;
+    uint32_t start = sphere_start_v(v, root, key, q, margin);
+    uint32_t w = find_reliable_v(v, root, start, key, q, [&](uint32_t) { ++reads; }, &e);
     status[i] = (w != INVALID) ? 1 : 2;
     witness[i] = w;
-    dleaf[i] = descent_leaf_v(v, root, key, q, &e);
+    cnt[i] = (w != INVALID) ? 1u : reads + 1u;
+    dleaf[i] = descent_leaf_v(v, root, start, key, q, &e);
     if (e) atomicExch(err, e);
 }
 
@@ -360,33 +419,34 @@ __global__ void k_waves_coop(uint32_t nf0, uint32_t *front, uint32_t *next, cons
         next = tmp;
         ++wave;
     }
-    if (gtid == 0) *waves_out = wave;
+    if (gtid == 0) *waves_out += wave;   // running total over the rounds
 }
 
 // Dependency lists: the leaves each pending side depends on (its witness if
-// reliable; the leaves its search read plus its descent leaf if a writer).
-// Phase 0 counts, phase 1 writes (leaf, side) pairs at `off`.
+// reliable; the leaves its search read plus its descent leaf if a writer),
+// written as (leaf, side) pairs at the offsets of the evaluation's counts.
 __global__ void k_sens(uint32_t m, const uint32_t *keys, NV v, Root root, const D3 *pos, const D3 *nrm,
                        const double *scale, double h_svo, const uint8_t *status, const uint32_t *witness,
-                       const uint32_t *dleaf, uint32_t *cnt, const uint32_t *off, uint32_t *skeys, uint32_t *svals,
-                       int phase, int *err) {
+                       const uint32_t *dleaf, const uint32_t *off, uint32_t *skeys, uint32_t *svals, double margin,
+                       int *err) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m) return;
     if (status[i] == 1) {
-        if (phase == 0) cnt[i] = 1;
-        else { skeys[off[i]] = witness[i]; svals[off[i]] = i; }
+        skeys[off[i]] = witness[i];
+        svals[off[i]] = i;
         return;
     }
     uint32_t key = keys[i];
     SampleRef q = sample_side(key, pos, nrm, scale, h_svo);
     int e = 0;
-    uint32_t c = 0, o = phase ? off[i] : 0;
-    find_reliable_v(v, root, key, q, [&](uint32_t leaf) {
-        if (phase) { skeys[o + c] = leaf; svals[o + c] = i; }
+    uint32_t c = 0, o = off[i];
+    find_reliable_v(v, root, sphere_start_v(v, root, key, q, margin), key, q, [&](uint32_t leaf) {
+        skeys[o + c] = leaf;
+        svals[o + c] = i;
         ++c;
     }, &e);
-    if (phase) { skeys[o + c] = dleaf[i]; svals[o + c] = i; }
-    else cnt[i] = c + 1;
+    skeys[o + c] = dleaf[i];
+    svals[o + c] = i;
     if (e) atomicExch(err, e);
 }
 
@@ -1025,8 +1085,11 @@ void build_tree(tsr_tree &t, const tsr_samples_view &sv, bool on_device) {
         seg_hi.alloc(S.cap, st);
         DBuf<unsigned long long> wcount(1, st);
         wcount.zero();
-        DBuf<uint32_t> counters(4, st);
+        DBuf<uint32_t> counters(4, st), waves_total(1, st);
+        waves_total.zero();
         uint32_t rounds = 0, waves = 0;
+        const double margin = 1e-12 * (std::max(std::max(std::fabs(root.mn.x), std::fabs(root.mn.y)),
+                                                 std::fabs(root.mn.z)) + 2.0 * root.size);
         float eval_ms = 0, resolve_ms = 0;
         cudaEvent_t e0, e1, e2;
         TSR_CUDA(cudaEventCreate(&e0)); TSR_CUDA(cudaEventCreate(&e1)); TSR_CUDA(cudaEventCreate(&e2));
@@ -1043,19 +1106,15 @@ void build_tree(tsr_tree &t, const tsr_samples_view &sv, bool on_device) {
             NV v = view(S);
             DBuf<uint8_t> status(m, st);
             DBuf<uint32_t> unres(m, st), witness(m, st), dleaf(m, st);
+            DBuf<uint32_t> scnt(m + 1, st), soff(m + 1, st), writers(m, st);
             unres.zero();
+            TSR_CUDA(cudaMemsetAsync(scnt.p + m, 0, 4, st));
             TSR_CUDA(cudaEventRecord(e0, st));
             k_sampling_eval<<<grid_for(m, 128), 128, 0, st>>>(m, keys.p, v, root, pos.p, nrm.p, scale.p, h_svo,
-                                                             status.p, witness.p, dleaf.p, derr.p); ::tsr::note_launch();
+                                                             status.p, witness.p, dleaf.p, scnt.p, margin, derr.p);
+            ::tsr::note_launch();
             TSR_CUDA(cudaEventRecord(e1, st));
-            if (int e0v = read_scalar(derr.p, st))
-                fail(TSR_ERR_DEVICE_ASSERT, "sampling evaluation invariant broken (code " + std::to_string(e0v) + ")");
             // dependency index (leaf -> sides) and the writer list
-            DBuf<uint32_t> scnt(m + 1, st), soff(m + 1, st), writers(m, st);
-            TSR_CUDA(cudaMemsetAsync(scnt.p + m, 0, 4, st));
-            k_sens<<<grid_for(m, 128), 128, 0, st>>>(m, keys.p, v, root, pos.p, nrm.p, scale.p, h_svo, status.p,
-                                                    witness.p, dleaf.p, scnt.p, nullptr, nullptr, nullptr, 0,
-                                                    derr.p); ::tsr::note_launch();
             exclusive_scan(scnt.p, soff.p, m + 1, st);
             counters.zero();
             k_writer_list<<<grid_for(m, BLK), BLK, 0, st>>>(m, status.p, writers.p, counters.p); ::tsr::note_launch();
@@ -1067,7 +1126,7 @@ void build_tree(tsr_tree &t, const tsr_samples_view &sv, bool on_device) {
             DBuf<uint32_t> skeys(nsens, st), svals(nsens, st), ssorted(nsens, st), by_leaf(nsens, st);
             if (nsens) {
                 k_sens<<<grid_for(m, 128), 128, 0, st>>>(m, keys.p, v, root, pos.p, nrm.p, scale.p, h_svo, status.p,
-                                                        witness.p, dleaf.p, nullptr, soff.p, skeys.p, svals.p, 1,
+                                                        witness.p, dleaf.p, soff.p, skeys.p, svals.p, margin,
                                                         derr.p); ::tsr::note_launch();
                 sort_pairs(skeys.p, ssorted.p, svals.p, by_leaf.p, nsens, st);
                 k_segments<<<grid_for(nsens, BLK), BLK, 0, st>>>(nsens, ssorted.p, seg_lo.p, seg_hi.p); ::tsr::note_launch();
@@ -1077,18 +1136,16 @@ void build_tree(tsr_tree &t, const tsr_samples_view &sv, bool on_device) {
             uint32_t nf = nwri;
             if (nwri) {
                 TSR_CUDA(cudaMemcpyAsync(front.p, writers.p, (size_t)nwri * 4, cudaMemcpyDeviceToDevice, st));
-                DBuf<uint32_t> ctr(4, st), waves_out(1, st);
+                DBuf<uint32_t> ctr(4, st);
                 ctr.zero();
                 uint32_t max_waves = 1u << 22;
                 uint32_t *fp = front.p, *np = next.p, *tp = touched.p, *kp = keys.p, *dp = dleaf.p, *mp = mark.p;
                 uint32_t *slp = seg_lo.p, *shp = seg_hi.p, *blp = by_leaf.p, *up = unres.p, *cp = ctr.p;
-                uint32_t *wp = waves_out.p;
+                uint32_t *wp = waves_total.p;
                 int *ep = derr.p;
                 void *args[] = {&nf, &fp, &np, &kp, &dp, &mp, &tp, &slp, &shp, &blp, &up, &cp, &max_waves, &wp, &ep};
                 TSR_CUDA(cudaLaunchCooperativeKernel((const void *)k_waves_coop, coop_grid, 256, args, 0, st));
                 ::tsr::note_launch();
-                waves += read_scalar(waves_out.p, st);
-                if (read_scalar(derr.p, st) == 7) fail(TSR_ERR_TIMEOUT, "sampling conflict resolution did not converge");
             }
             TSR_CUDA(cudaEventRecord(e2, st));
             if (nsens) k_segments_clear<<<grid_for(nsens, BLK), BLK, 0, st>>>(nsens, ssorted.p, seg_lo.p); ::tsr::note_launch();
@@ -1131,11 +1188,15 @@ void build_tree(tsr_tree &t, const tsr_samples_view &sv, bool on_device) {
         }
         cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(e2);
         t.sampling_rounds = rounds;
-        t.sampling_waves = waves;
         t.stage_ms[6] = eval_ms;
         t.stage_ms[7] = resolve_ms;
         t.sampling_writers = read_scalar(wcount.p, st);
+        waves = read_scalar(waves_total.p, st);
+        t.sampling_waves = waves;
+        // device-side failures of any round are reported once the rounds end
+        // (every index a failing round leaves behind is still in range)
         int e = read_scalar(derr.p, st);
+        if (e == 7) fail(TSR_ERR_TIMEOUT, "sampling conflict resolution did not converge");
         if (e) fail(TSR_ERR_DEVICE_ASSERT, "sampling traversal invariant broken (code " + std::to_string(e) + ")");
     }
     t.stage_ms[1] = timer.lap();
