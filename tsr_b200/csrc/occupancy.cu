@@ -41,9 +41,10 @@ __device__ inline float fdot(F3 a, F3 b) { return a.x * b.x + a.y * b.y + a.z * 
 // te = dot(x - end, m) / denom = tComplete - 1, which keeps the arithmetic
 // near the sample (where the kernels are evaluated) well conditioned.
 struct ConeF {
-    F3 apex, end, axis, m;   // m = end-disc normal
-    float radius, full, length, inv_denom, a_over_l, t_start_e;
-    float n1, sqrt3_slack;
+    F3 end, axis, m;   // m = end-disc normal
+    float radius, full, inv_denom, a_over_l, t_start_e;
+    float ray_k;       // 3 / (2 L), L = cone length
+    float n1;          // |m|_1
 };
 
 struct LinkIn {
@@ -61,33 +62,29 @@ struct TreeIn {
 
 
 // Occupancy::addKernel (Occupancy.cpp:279-346) at a leaf centre x, given
-// te = dot(x - end, m) / denom (= tComplete - 1) and r2 = |x - PCD centre|^2.
-__device__ inline bool kernel_at(const ConeF &c, float te, float r2, bool sampleness, float conf, float *out) {
-    float tcut_m1 = te * c.a_over_l;               // tCut - 1
-    float tcut = 1.0f + tcut_m1;
-    if (tcut < 0.0f || tcut >= 1.0f) return false;
-    float tc = 1.0f + te;
-    float pr = c.radius * tc;
-    float pr2 = pr * pr;
-    if (r2 >= pr2) return false;
-    float ray;
-    if (!sampleness) {
-        // Z = L, z = tCut Z: 3/(2Z) (1 - tCut^2) = 3/(2Z) (1 - tCut)(1 + tCut)
-        float Z = c.length;
-        ray = (1.5f / Z) * ((-tcut_m1) * (1.0f + tcut));
+// te = dot(x - end, m) / denom (= tComplete - 1) and r2 = |x - PCD centre|^2:
+// the confidence-scaled kernel value, or 0 where addKernel adds nothing.
+// Straight-line code (no early exits), so that the lanes of a warp testing
+// different children stay together.
+__device__ __forceinline__ float kernel_value(const ConeF &c, float te, float r2, bool sampleness, float conf) {
+    const float tcut_m1 = te * c.a_over_l;         // tCut - 1
+    const float tcut = 1.0f + tcut_m1;
+    const float pr = c.radius * (1.0f + te);       // PCD radius at tComplete
+    const float pr2 = pr * pr;
+    bool ok = (tcut >= 0.0f) & (tcut < 1.0f) & (r2 < pr2);
+    float f;   // ray factor: 3/(2Z)(1 - (z/Z)^2) with the 3/(2 L) part in ray_k
+    if (sampleness) {
+        const float tcen = fabsf(tcut - 0.5f) * 2.0f;
+        f = 1.0f - tcen * tcen;
+        ok &= tcen < 1.0f;
     } else {
-        float tcen = fabsf(tcut - 0.5f) * 2.0f;
-        float Z = 0.5f * c.length;
-        if (tcen >= 1.0f) return false;
-        ray = (1.5f / Z) * (1.0f - tcen * tcen) * 0.5f;
+        f = (-tcut_m1) * (1.0f + tcut);            // (1 - tCut)(1 + tCut)
     }
-    float disc = (0.63661977236758134f / pr2) * (1.0f - r2 / pr2);
-    float kv = ray * disc;
-    if (!(kv >= (float)EPS)) return false;
-    float scaled = conf * kv;
-    if (!(scaled >= (float)EPS)) return false;
-    *out = scaled;
-    return true;
+    const float inv = __frcp_rn(pr2);
+    const float kv = c.ray_k * f * (0.63661977236758134f * inv) * (1.0f - r2 * inv);
+    const float scaled = conf * kv;
+    ok &= (kv >= (float)EPS) & (scaled >= (float)EPS);
+    return ok ? scaled : 0.0f;
 }
 
 // Cone-frame coordinates of point x: te and the squared distance to the axis.
@@ -98,10 +95,10 @@ __device__ __forceinline__ void cone_coords(const ConeF &c, F3 x, float &te, flo
     r2 = fdot(q, q);
 }
 
-__device__ inline bool eval_kernel(const ConeF &c, F3 x, bool sampleness, float conf, float *out) {
+__device__ inline float eval_kernel(const ConeF &c, F3 x, bool sampleness, float conf) {
     float te, r2;
     cone_coords(c, x, te, r2);
-    return kernel_at(c, te, r2, sampleness, conf, out);
+    return kernel_value(c, te, r2, sampleness, conf);
 }
 
 __device__ inline F3 rel(const D3 &a, const D3 &origin) {
@@ -134,15 +131,15 @@ __device__ inline bool cone_box_separated_pt(const ConeF &c, F3 bmin, float size
 
 // The same test for a box of centre coordinates (te, r2) and half size hs
 // already widened by the recurrence slack; dt = hs * |m|_1 * |1/denom|.
+// The last comparison, qn - 1e-4 qn > k with qn = sqrt(r2), is taken on
+// squares (k > 0 whenever it is reached).  Straight-line code.
 __device__ __forceinline__ bool separated_at(const ConeF &c, float te, float r2, float hs, float dt) {
-    float slack = 1e-4f * (dt + fabsf(te)) + 1e-6f;
-    if (te + dt < c.t_start_e - slack) return true;
-    if (te - dt >= slack) return true;
-    if (1.0f + te + dt <= 0.0f) return true;
-    float qn = sqrtf(r2);
-    float tmax = fminf(1.0f + te + dt, 1.0f);
-    float bound = qn - hs * 1.7320508f - dt * c.full;
-    return bound > tmax * c.radius * 1.0001f + 1e-4f * (qn + hs + dt * c.full);
+    const float slack = 1e-4f * (dt + fabsf(te)) + 1e-6f;
+    bool sep = (te + dt < c.t_start_e - slack) | (te - dt >= slack) | (1.0f + te + dt <= 0.0f);
+    const float tmax = fminf(1.0f + te + dt, 1.0f);
+    const float k = hs * 1.7320508f + dt * c.full + tmax * c.radius * 1.0001f + 1e-4f * (hs + dt * c.full);
+    sep |= (k > 0.0f) & (r2 * 0.99980001f > k * k);
+    return sep;
 }
 
 constexpr int PT_BLOCK = 128;
@@ -183,15 +180,169 @@ __device__ __forceinline__ F3 child_min(F3 pmin, uint32_t ci, float size) {
               (ci & 4u) ? pmin.z + size : pmin.z);
 }
 
+// Per-link set-up of the traversal, precomputed by one thread per link so
+// that the persistent traversal below never runs this long FP64 stretch for a
+// few lanes of a warp while the others wait.  c0 == INVALID: nothing to
+// traverse (no camera, degenerated cone, pruned start, or a start leaf that
+// the set-up kernel has already visited).
+struct __align__(16) LinkRec {
+    float end[3], axis[3], m[3];
+    float radius, full, ray_k, inv_denom, a_over_l, t_start_e, n1;
+    float smin[3], fconf;     // start node corner in the sample's frame; confidence
+    double wlen;              // confidence * cone length
+    uint32_t c0;              // children block of the start node
+    uint32_t depths;          // depth of those children | max depth << 8
+    double spos[3];           // the sample: origin of the FP32 frame
+    uint64_t pad;
+};
+
+__device__ __forceinline__ ConeF cone_of(const LinkRec &r) {
+    ConeF c;
+    c.end = f3(r.end[0], r.end[1], r.end[2]);
+    c.axis = f3(r.axis[0], r.axis[1], r.axis[2]);
+    c.m = f3(r.m[0], r.m[1], r.m[2]);
+    c.radius = r.radius;
+    c.full = r.full;
+    c.ray_k = r.ray_k;
+    c.inv_denom = r.inv_denom;
+    c.a_over_l = r.a_over_l;
+    c.t_start_e = r.t_start_e;
+    c.n1 = r.n1;
+    return c;
+}
+
+// Set-up of link order[i] (Occupancy.cpp:174-201), FP64, and the start of its
+// traversal: the deepest node containing the cut cone's bounding box.
 template <int TYPE>
-__global__ void __launch_bounds__(PT_BLOCK, (TYPE == 0) ? 6 : 5) k_cone_x(uint64_t nlinks, const uint32_t *order, LinkIn in,
-                                                        TreeIn tr, const uint2 *rec, double *ksum, double *clen,
-                                                        double *cone_count, unsigned long long *accepted,
-                                                        unsigned long long *next_link, unsigned long long *visits,
-                                                        int *err) {
+__global__ void __launch_bounds__(128) k_link_setup(uint64_t nlinks, const uint32_t *order, LinkIn in, TreeIn tr,
+                                                    const uint2 *rec, LinkRec *out, double *ksum, double *clen,
+                                                    double *cone_count, unsigned long long *accepted) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    double count = 0.0;
+    unsigned long long acc = 0;
+    if (i < nlinks) {
+        LinkRec r;
+        r.c0 = INVALID;
+        r.depths = 0;
+        do {
+            uint64_t l = order ? order[i] : i;
+            uint32_t s = (uint32_t)(l / in.k);
+            uint32_t cam = in.links[l];
+            if (cam == INVALID || cam >= in.ncams) break;
+            D3 p = in.pos[s];
+            D3 n = in.nrm[s];
+            D3 cwp = in.cams[cam];
+            double kernel_r = in.h_o * in.scale[s];
+            D3 apex_d{cwp.x - p.x, cwp.y - p.y, cwp.z - p.z};
+            D3 end_d{0.0, 0.0, 0.0};
+            double cone_len = REAL_MAX;
+            if (TYPE == SAMPLENESS) {
+                D3 cs{-apex_d.x, -apex_d.y, -apex_d.z};
+                double total = sqrt(cs.x * cs.x + cs.y * cs.y + cs.z * cs.z);
+                cone_len = kernel_r * in.rel_cone;
+                double hh = cone_len * 0.5;
+                end_d = D3{cs.x / total * hh, cs.y / total * hh, cs.z / total * hh};
+            }
+            D3 m{-n.x, -n.y, -n.z};
+            D3 axis{end_d.x - apex_d.x, end_d.y - apex_d.y, end_d.z - apex_d.z};
+            double full = sqrt(axis.x * axis.x + axis.y * axis.y + axis.z * axis.z);
+            double length = cone_len < full ? cone_len : full;
+            double denom = axis.x * m.x + axis.y * m.y + axis.z * m.z;
+            if (!(full > EPS) || !(kernel_r > 0.0) || fabs(denom) <= EPS * full) break;   // isDegenerated
+            double conf = in.conf[s];
+            if (TYPE == EMPTINESS) count += conf;
+            const double wlen = conf * length;
+            const float fconf = (float)conf;
+            const uint32_t max_depth =
+                (uint32_t)ceil(log2(in.root_size / (in.scale[s] * in.h_svo))) + MAX_DEPTH_DIFFERENCE;
+            ConeF c;
+            c.end = f3((float)end_d.x, (float)end_d.y, (float)end_d.z);
+            c.axis = f3((float)axis.x, (float)axis.y, (float)axis.z);
+            c.m = f3((float)m.x, (float)m.y, (float)m.z);
+            c.radius = (float)kernel_r;
+            c.full = (float)full;
+            c.ray_k = (float)(1.5 / length);
+            c.inv_denom = (float)(1.0 / denom);
+            c.a_over_l = (float)(full / length);
+            c.t_start_e = (float)(-length / full);
+            c.n1 = fabsf(c.m.x) + fabsf(c.m.y) + fabsf(c.m.z);
+            F3 p0 = c.end + c.axis * c.t_start_e;
+            F3 lo = f3(fminf(p0.x, c.end.x) - c.radius, fminf(p0.y, c.end.y) - c.radius, fminf(p0.z, c.end.z) - c.radius);
+            F3 hi = f3(fmaxf(p0.x, c.end.x) + c.radius, fmaxf(p0.y, c.end.y) + c.radius, fmaxf(p0.z, c.end.z) + c.radius);
+            const float root_size_f = (float)in.root_size;
+            uint32_t start = 0, base = 0;
+            uint2 srec = __ldg(&rec[REC_OFFSET]);
+            F3 smin = rel(tr.nmin[0], p);
+            float ssize = root_size_f;
+            while (srec.x != INVALID && base + 1 <= max_depth) {
+                float cs = 0.5f * ssize;
+                float margin = 1e-5f * ssize;
+                F3 ctr = smin + f3(cs, cs, cs);
+                const float l3[3] = {lo.x, lo.y, lo.z}, h3[3] = {hi.x, hi.y, hi.z}, c3[3] = {ctr.x, ctr.y, ctr.z};
+                uint32_t digit = 0;
+                bool inside = true;
+                for (int a = 0; a < 3; ++a) {
+                    if (h3[a] < c3[a] - margin) continue;
+                    if (l3[a] > c3[a] + margin) { digit |= 1u << a; continue; }
+                    inside = false;
+                }
+                if (!inside) break;
+                start = srec.x + digit;
+                srec = __ldg(&rec[start + REC_OFFSET]);
+                smin = rel(tr.nmin[start], p);
+                ssize = cs;
+                ++base;
+            }
+            if (TYPE == EMPTINESS && !(srec.y & REC_FLAG)) break;
+            if (cone_box_separated_pt(c, smin, ssize)) break;
+            if (srec.x == INVALID) {   // the start is a leaf: visit it here
+                float h = 0.5f * ssize;
+                float val = eval_kernel(c, smin + f3(h, h, h), TYPE == SAMPLENESS, fconf);
+                if (val > 0.0f) {
+                    uint32_t leaf = srec.y & REC_NOLEAF;
+                    atomicAdd(&ksum[leaf], (double)val);
+                    atomicAdd(&clen[leaf], wlen);
+                    ++acc;
+                }
+                break;
+            }
+            if (base + 1 > max_depth) break;
+            r.end[0] = c.end.x; r.end[1] = c.end.y; r.end[2] = c.end.z;
+            r.axis[0] = c.axis.x; r.axis[1] = c.axis.y; r.axis[2] = c.axis.z;
+            r.m[0] = c.m.x; r.m[1] = c.m.y; r.m[2] = c.m.z;
+            r.radius = c.radius; r.full = c.full; r.ray_k = c.ray_k; r.inv_denom = c.inv_denom;
+            r.a_over_l = c.a_over_l; r.t_start_e = c.t_start_e; r.n1 = c.n1;
+            r.smin[0] = smin.x; r.smin[1] = smin.y; r.smin[2] = smin.z;
+            r.fconf = fconf;
+            r.wlen = wlen;
+            r.c0 = srec.x;
+            r.depths = (base + 1) | (max_depth << 8);
+            r.spos[0] = p.x; r.spos[1] = p.y; r.spos[2] = p.z;
+            r.pad = 0;
+        } while (0);
+        out[i] = r;
+    }
+    typedef cub::BlockReduce<double, 128> BR;
+    typedef cub::BlockReduce<unsigned long long, 128> BRU;
+    __shared__ typename BR::TempStorage tmp;
+    __shared__ typename BRU::TempStorage tmpu;
+    double bc = BR(tmp).Sum(count);
+    unsigned long long ba = BRU(tmpu).Sum(acc);
+    if (threadIdx.x == 0) {
+        if (TYPE == EMPTINESS && bc != 0.0) atomicAdd(cone_count, bc);
+        if (ba) atomicAdd(accepted, ba);
+    }
+}
+
+template <int TYPE>
+__global__ void __launch_bounds__(PT_BLOCK, (TYPE == 0) ? 6 : 5) k_cone_x(uint64_t nlinks, const LinkRec *links,
+                                                                         TreeIn tr, const uint2 *rec,
+                                                                         float root_size_f, double *ksum,
+                                                                         double *clen, unsigned long long *accepted,
+                                                                         unsigned long long *next_link,
+                                                                         unsigned long long *visits, int *err) {
     const unsigned FULL = 0xffffffffu;
     const unsigned lane = threadIdx.x & 31;
-    const float root_size_f = (float)in.root_size;
     // stack of expanded nodes that still have children to descend into
     uint64_t st[MAX_TREE_DEPTH];   // children block | mask << 32 | depth << 40
     int sp = 0;
@@ -205,17 +356,7 @@ __global__ void __launch_bounds__(PT_BLOCK, (TYPE == 0) ? 6 : 5) k_cone_x(uint64
     double wlen = 0.0;
     float fconf = 0.f;
     bool done = false;
-    double count = 0.0;
     unsigned long long acc = 0, nvis = 0;
-
-    auto visit_leaf = [&](uint32_t leaf, F3 bmin, float size) {
-        float h = 0.5f * size;
-        float val;
-        if (!eval_kernel(c, bmin + f3(h, h, h), TYPE == SAMPLENESS, fconf, &val)) return;
-        atomicAdd(&ksum[leaf], (double)val);
-        atomicAdd(&clen[leaf], wlen);
-        ++acc;
-    };
 
     while (true) {
         // resume the deepest expanded node that has children left
@@ -241,85 +382,20 @@ __global__ void __launch_bounds__(PT_BLOCK, (TYPE == 0) ? 6 : 5) k_cone_x(uint64
                 uint64_t i = b + __popc(nm & ((1u << lane) - 1u));
                 if (i >= nlinks) {
                     done = true;
-                } else do {
-                    // ---- set-up of link l (Occupancy.cpp:174-201), FP64
-                    uint64_t l = order ? order[i] : i;
-                    uint32_t s = (uint32_t)(l / in.k);
-                    uint32_t cam = in.links[l];
-                    if (cam == INVALID || cam >= in.ncams) break;
-                    D3 p = in.pos[s];
-                    spos = p;
-                    D3 n = in.nrm[s];
-                    D3 cwp = in.cams[cam];
-                    double kernel_r = in.h_o * in.scale[s];
-                    D3 apex_d{cwp.x - p.x, cwp.y - p.y, cwp.z - p.z};
-                    D3 end_d{0.0, 0.0, 0.0};
-                    double cone_len = REAL_MAX;
-                    if (TYPE == SAMPLENESS) {
-                        D3 cs{-apex_d.x, -apex_d.y, -apex_d.z};
-                        double total = sqrt(cs.x * cs.x + cs.y * cs.y + cs.z * cs.z);
-                        cone_len = kernel_r * in.rel_cone;
-                        double hh = cone_len * 0.5;
-                        end_d = D3{cs.x / total * hh, cs.y / total * hh, cs.z / total * hh};
+                } else {
+                    const LinkRec r = links[i];
+                    if (r.c0 != INVALID) {
+                        c = cone_of(r);
+                        wlen = r.wlen;
+                        fconf = r.fconf;
+                        max_depth = r.depths >> 8;
+                        spos = D3{r.spos[0], r.spos[1], r.spos[2]};
+                        x_c0 = r.c0;
+                        x_min = f3(r.smin[0], r.smin[1], r.smin[2]);
+                        x_d = r.depths & 0xFFu;
+                        have = true;
                     }
-                    D3 m{-n.x, -n.y, -n.z};
-                    D3 axis{end_d.x - apex_d.x, end_d.y - apex_d.y, end_d.z - apex_d.z};
-                    double full = sqrt(axis.x * axis.x + axis.y * axis.y + axis.z * axis.z);
-                    double length = cone_len < full ? cone_len : full;
-                    double denom = axis.x * m.x + axis.y * m.y + axis.z * m.z;
-                    if (!(full > EPS) || !(kernel_r > 0.0) || fabs(denom) <= EPS * full) break;   // isDegenerated
-                    double conf = in.conf[s];
-                    if (TYPE == EMPTINESS) count += conf;
-                    wlen = conf * length;
-                    fconf = (float)conf;
-                    max_depth = (uint32_t)ceil(log2(in.root_size / (in.scale[s] * in.h_svo))) + MAX_DEPTH_DIFFERENCE;
-                    c.apex = f3((float)apex_d.x, (float)apex_d.y, (float)apex_d.z);
-                    c.end = f3((float)end_d.x, (float)end_d.y, (float)end_d.z);
-                    c.axis = f3((float)axis.x, (float)axis.y, (float)axis.z);
-                    c.m = f3((float)m.x, (float)m.y, (float)m.z);
-                    c.radius = (float)kernel_r;
-                    c.full = (float)full;
-                    c.length = (float)length;
-                    c.inv_denom = (float)(1.0 / denom);
-                    c.a_over_l = (float)(full / length);
-                    c.t_start_e = (float)(-length / full);
-                    c.n1 = fabsf(c.m.x) + fabsf(c.m.y) + fabsf(c.m.z);
-                    // start at the deepest node containing the cut cone's bounding box
-                    F3 p0 = c.end + c.axis * c.t_start_e;
-                    F3 lo = f3(fminf(p0.x, c.end.x) - c.radius, fminf(p0.y, c.end.y) - c.radius, fminf(p0.z, c.end.z) - c.radius);
-                    F3 hi = f3(fmaxf(p0.x, c.end.x) + c.radius, fmaxf(p0.y, c.end.y) + c.radius, fmaxf(p0.z, c.end.z) + c.radius);
-                    uint32_t start = 0, base = 0;
-                    uint2 srec = __ldg(&rec[REC_OFFSET]);
-                    F3 smin = rel(tr.nmin[0], p);
-                    float ssize = root_size_f;
-                    while (srec.x != INVALID && base + 1 <= max_depth) {
-                        float cs = 0.5f * ssize;
-                        float margin = 1e-5f * ssize;
-                        F3 ctr = smin + f3(cs, cs, cs);
-                        const float l3[3] = {lo.x, lo.y, lo.z}, h3[3] = {hi.x, hi.y, hi.z}, c3[3] = {ctr.x, ctr.y, ctr.z};
-                        uint32_t digit = 0;
-                        bool inside = true;
-                        for (int a = 0; a < 3; ++a) {
-                            if (h3[a] < c3[a] - margin) continue;
-                            if (l3[a] > c3[a] + margin) { digit |= 1u << a; continue; }
-                            inside = false;
-                        }
-                        if (!inside) break;
-                        start = srec.x + digit;
-                        srec = __ldg(&rec[start + REC_OFFSET]);
-                        smin = rel(tr.nmin[start], p);
-                        ssize = cs;
-                        ++base;
-                    }
-                    if (TYPE == EMPTINESS && !(srec.y & REC_FLAG)) break;
-                    if (cone_box_separated_pt(c, smin, ssize)) break;
-                    if (srec.x == INVALID) { visit_leaf(srec.y & REC_NOLEAF, smin, ssize); break; }
-                    if (base + 1 > max_depth) break;
-                    x_c0 = srec.x;
-                    x_min = smin;
-                    x_d = base + 1;
-                    have = true;
-                } while (0);
+                }
             }
         }
         if (__all_sync(FULL, done && !have && sp == 0)) break;
@@ -346,23 +422,24 @@ __global__ void __launch_bounds__(PT_BLOCK, (TYPE == 0) ? 6 : 5) k_cone_x(uint64
         nvis += 8;
 #pragma unroll
         for (int ci = 0; ci < 8; ++ci) {
-            if (TYPE == EMPTINESS && !(ry[ci] & REC_FLAG)) continue;
+            // both tests for every child, without branches; only the outcome
+            // (a leaf's kernel, or a child to descend into) is conditional
+            const bool flagged = TYPE == SAMPLENESS || (ry[ci] & REC_FLAG);
+            const bool leaf = rx[ci] == INVALID;
             F3 ctr = f3((ci & 1) ? ctr0.x + size : ctr0.x, (ci & 2) ? ctr0.y + size : ctr0.y,
                         (ci & 4) ? ctr0.z + size : ctr0.z);
             float te, r2;
             cone_coords(c, ctr, te, r2);
-            if (rx[ci] == INVALID) {
-                // a leaf: addKernel's exact test decides, no box test needed
-                float val;
-                if (kernel_at(c, te, r2, TYPE == SAMPLENESS, fconf, &val)) {
-                    uint32_t leaf = ry[ci] & REC_NOLEAF;
-                    atomicAdd(&ksum[leaf], (double)val);
-                    atomicAdd(&clen[leaf], wlen);
-                    ++acc;
-                }
-            } else if (can_descend && !separated_at(c, te, r2, hs, dt)) {
-                mask |= 1u << ci;
+            const float val = kernel_value(c, te, r2, TYPE == SAMPLENESS, fconf);
+            const bool sep = separated_at(c, te, r2, hs, dt);
+            // a leaf: addKernel's exact test decides, no box test needed
+            if (flagged && leaf && val > 0.0f) {
+                uint32_t lf = ry[ci] & REC_NOLEAF;
+                atomicAdd(&ksum[lf], (double)val);
+                atomicAdd(&clen[lf], wlen);
+                ++acc;
             }
+            if (flagged && !leaf && can_descend && !sep) mask |= 1u << ci;
         }
         if (mask) {
             uint32_t ci = __ffs(mask) - 1;
@@ -385,12 +462,10 @@ __global__ void __launch_bounds__(PT_BLOCK, (TYPE == 0) ? 6 : 5) k_cone_x(uint64
         }
     }
     for (int o = 16; o; o >>= 1) {
-        count += __shfl_xor_sync(FULL, count, o);
         acc += __shfl_xor_sync(FULL, acc, o);
         nvis += __shfl_xor_sync(FULL, nvis, o);
     }
     if (lane == 0) {
-        if (TYPE == EMPTINESS && count != 0.0) atomicAdd(cone_count, count);
         if (acc) atomicAdd(accepted, acc);
         if (nvis) atomicAdd(visits, nvis);
     }
@@ -707,7 +782,11 @@ void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_
     if (reinterpret_cast<uintptr_t>(recs.p) % 16) fail(TSR_ERR_CUDA, "traversal records are not 16-byte aligned");
     next_link.zero();
     k_pack_rec<<<grid_for(nn, BLK), BLK, 0, st>>>(nn, t.children.p, t.node_to_leaf.p, nullptr, recs.p); ::tsr::note_launch();
-    k_cone_x<SAMPLENESS><<<x_grid, PT_BLOCK, 0, st>>>(nlinks, nullptr, in, tr, recs.p, ssum, slen, cone_count.p,
+    DBuf<LinkRec> lrec((size_t)nlinks, st);
+    k_link_setup<SAMPLENESS><<<grid_for(nlinks, 128), 128, 0, st>>>(nlinks, nullptr, in, tr, recs.p, lrec.p, ssum,
+                                                                    slen, cone_count.p, accepted.p + 1);
+    ::tsr::note_launch();
+    k_cone_x<SAMPLENESS><<<x_grid, PT_BLOCK, 0, st>>>(nlinks, lrec.p, tr, recs.p, (float)t.root_size, ssum, slen,
                                                      accepted.p + 1, next_link.p, accepted.p + 3, err.p);
     ::tsr::note_launch();
     k_leaf_flags<<<grid_for(nl, BLK), BLK, 0, st>>>(nl, t.leaf_node.p, ssum, o.states.p, FLAG_SAMPLENESS); ::tsr::note_launch();
@@ -734,7 +813,10 @@ void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_
     k_pack_rec<<<grid_for(nn, BLK), BLK, 0, st>>>(nn, t.children.p, t.node_to_leaf.p, o.states.p, recs.p); ::tsr::note_launch();
     o.stage_ms[1] = timer.lap();
     next_link.zero();
-    k_cone_x<EMPTINESS><<<x_grid, PT_BLOCK, 0, st>>>(nlinks, order.p, in, tr, recs.p, esum, elen, cone_count.p,
+    k_link_setup<EMPTINESS><<<grid_for(nlinks, 128), 128, 0, st>>>(nlinks, order.p, in, tr, recs.p, lrec.p, esum,
+                                                                   elen, cone_count.p, accepted.p);
+    ::tsr::note_launch();
+    k_cone_x<EMPTINESS><<<x_grid, PT_BLOCK, 0, st>>>(nlinks, lrec.p, tr, recs.p, (float)t.root_size, esum, elen,
                                                     accepted.p, next_link.p, accepted.p + 2, err.p);
     ::tsr::note_launch();
     k_leaf_flags<<<grid_for(nl, BLK), BLK, 0, st>>>(nl, t.leaf_node.p, esum, o.states.p, FLAG_EMPTINESS); ::tsr::note_launch();
