@@ -538,6 +538,17 @@ __global__ void k_prior_sums(uint32_t lo, uint32_t hi, uint32_t nn, const uint32
     }
 }
 
+// intersectAABBWithSphere as the tree build evaluates it (aabb_sphere), with
+// the per-axis branches turned into selects: an axis where the centre lies
+// within the box adds an exact +0, so the sum is bit-identical.
+__device__ __forceinline__ bool sphere_meets_box(const D3 &mn, const D3 &mx, const D3 &c, double r) {
+    const double tx = c.x < mn.x ? dsub(c.x, mn.x) : (c.x > mx.x ? dsub(c.x, mx.x) : 0.0);
+    const double ty = c.y < mn.y ? dsub(c.y, mn.y) : (c.y > mx.y ? dsub(c.y, mx.y) : 0.0);
+    const double tz = c.z < mn.z ? dsub(c.z, mn.z) : (c.z > mx.z ? dsub(c.z, mx.z) : 0.0);
+    const double d2 = dadd(dadd(dmul(tx, tx), dmul(ty, ty)), dmul(tz, tz));
+    return d2 <= dmul(r, r);
+}
+
 // Box entirely inside the sphere, with a strict relative margin so that every
 // leaf below certainly passes the closed sphere/box test.
 __device__ inline bool box_inside_sphere(const D3 &mn, double sz, const D3 &c, double r) {
@@ -658,17 +669,16 @@ __global__ void __launch_bounds__(PT_BLOCK) k_priors_x(uint32_t nl, uint32_t nn,
         if (d <= max_depth) {
 #pragma unroll
             for (int ci = 0; ci < 8; ++ci) {
-                if (!(ry[ci] & REC_FLAG)) continue;
-                D3 bmn = child_coords(x_min, cs, (uint32_t)ci);
-                D3 bmx{dadd(bmn.x, cs), dadd(bmn.y, cs), dadd(bmn.z, cs)};
-                if (!aabb_sphere(bmn, bmx, center, radius)) continue;
-                if (can_add && box_inside_sphere(bmn, cs, center, radius)) {
-                    add_row(x_c0 + ci, max_depth - d);
-                } else if (rx[ci] == INVALID) {
-                    add_row(x_c0 + ci, 0);
-                } else if (can_descend) {
-                    mask |= 1u << ci;
-                }
+                // every test for every child, without branches; only the
+                // outcome (a row to add, or a child to descend into) is conditional
+                const bool flagged = (ry[ci] & REC_FLAG) != 0;
+                const bool leaf = rx[ci] == INVALID;
+                const D3 bmn = child_coords(x_min, cs, (uint32_t)ci);
+                const D3 bmx{dadd(bmn.x, cs), dadd(bmn.y, cs), dadd(bmn.z, cs)};
+                const bool meets = flagged && sphere_meets_box(bmn, bmx, center, radius);
+                const bool inside = can_add && box_inside_sphere(bmn, cs, center, radius);
+                if (meets && (inside || leaf)) add_row(x_c0 + ci, inside ? max_depth - d : 0u);
+                if (meets && !inside && !leaf && can_descend) mask |= 1u << ci;
             }
         }
         if (mask) {
