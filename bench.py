@@ -35,22 +35,33 @@ sys.path.insert(0, str(ROOT))
 METRIC = "samples/s (octree+occupancy+DMC) MLP-pruned vs plain FP32 on B200, fixed mesh error"
 UNIT = "samples/s"
 L2_BYTES = 126 * 1024 * 1024
+# DRAM bytes per unit (per link for the cone passes, per leaf for the priors),
+# from the ncu capture summarised in profiles/occupancy_kernels_csg1m.md
+TRAFFIC_PER_UNIT = {"occ.sampleness": 159.9, "occ.emptiness": 161.4, "occ.priors": 220.9}
 CPU_SAMPLE_N = 60_000
+
+
+WORKLOADS = {
+    "csg4m": ("csg: 2 mm plate + cylinder r=0.3 + torus R=0.5/r=0.1, 120 cameras at 1.5-12, 4M samples",
+              4_000_000),
+    "csg1m": ("csg (as csg4m) subsampled to 1M samples, for profiling", 1_000_000),
+    "sphere": ("unit sphere, 24 cameras, ~250k samples", 250_000),
+    "heldout16m": ("held-out random CSG scene, 16M samples", 16_000_000),
+}
 
 
 def make_scene(workload, seed):
     from tsr_b200 import scenes
+    desc = WORKLOADS[workload][0]
     if workload == "csg4m":
-        return scenes.csg_scene(seed=seed, n_target=4_000_000), \
-            "csg: 2 mm plate + cylinder r=0.3 + torus R=0.5/r=0.1, 120 cameras at 1.5-12, 4M samples"
+        return scenes.csg_scene(seed=seed, n_target=4_000_000), desc
     if workload == "csg1m":
-        return scenes.csg_scene(seed=seed, n_target=1_000_000), \
-            "csg (as csg4m) subsampled to 1M samples, for profiling"
+        return scenes.csg_scene(seed=seed, n_target=1_000_000), desc
     if workload == "sphere":
-        return scenes.sphere_scene(seed=seed, stride=3), "unit sphere, 24 cameras, ~250k samples"
+        return scenes.sphere_scene(seed=seed, stride=3), desc
     if workload == "heldout16m":
-        return scenes.random_csg_scene(seed=999 + seed, n_target=16_000_000, width=1600, height=1200, f=1200.0), \
-            "held-out random CSG scene, 16M samples"
+        return scenes.random_csg_scene(seed=999 + seed, n_target=16_000_000, width=1600, height=1200,
+                                       f=1200.0), desc
     raise SystemExit("unknown workload " + workload)
 
 
@@ -152,12 +163,14 @@ def reference_arm(args):
     times = [run_oracle_once(scene, threads) for _ in range(args.steps)]
     t = sum(times)
     value = scene.n * args.steps / t
-    sample = "oracle full pipeline (tree, occupancy, priors, DMC) on the %s workload's geometry and cameras " \
-             "at %d samples" % (args.workload, scene.n)
+    sample = "each step: the oracle's full pipeline (tree, occupancy, priors, DMC) on %d samples of the " \
+             "same geometry and cameras, a bounded sample of the workload" % scene.n
+    desc, full_n = WORKLOADS[args.workload]
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": {"workload": args.workload, "samples": scene.n},
+            "data": "synthetic",
+            "config": {"workload": desc, "samples": full_n, "samples_per_timed_step": scene.n},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -250,11 +263,14 @@ def our_arm(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    # the clock sampler starts before the warm-up: its start-up (nvidia-smi
+    # initialising NVML) stalls CUDA calls briefly and must not land in a
+    # timed step; it keeps sampling through the timed region
+    clocks = Clocks(local)
+    clocks.start()
     for _ in range(args.warmup):
         device_step()
     # ---- timed: value (device-resident inputs)
-    clocks = Clocks(local)
-    clocks.start()
     barrier()
     l0 = core.kernel_launches()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
@@ -267,21 +283,26 @@ def our_arm(args):
     barrier()
     launches = core.kernel_launches() - l0
     clk = clocks.stop()
-    t_value = sum(a.elapsed_time(b) for a, b in ev) / 1e3
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    t_value = sum(step_ms) / 1e3
     t_value = max_over_ranks(t_value)
 
     # ---- timed: e2e through the public API from pinned host buffers
     h2d = n * (24 + 24 + 8 + 8 + 4 * scene.k) + scene.cams.nbytes
-    t_e2e, d2h = None, 0
+    t_e2e, d2h, e2e_step_ms = None, 0, []
     if not args.value_only:
         for _ in range(max(1, args.warmup // 2)):
             e2e_step()
         barrier()
-        t0 = time.perf_counter()
-        for _ in range(args.steps):
+        eev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(args.steps)]
+        for i in range(args.steps):
+            eev[i][0].record(stream)
             tree, mesh = e2e_step()
+            eev[i][1].record(stream)
         barrier()
-        t_e2e = max_over_ranks(time.perf_counter() - t0)
+        e2e_step_ms = [a.elapsed_time(b) for a, b in eev]
+        t_e2e = max_over_ranks(sum(e2e_step_ms) / 1e3)
         d2h = mesh.cases.nbytes + mesh.positions.nbytes + mesh.scales.nbytes + mesh.edge_keys.nbytes + \
             mesh.triangles.nbytes
 
@@ -297,6 +318,13 @@ def our_arm(args):
     alg = {"occ.sampleness": per_pass, "occ.emptiness": per_pass, "occ.priors": Nl * (16 + 8),
            "occ.finalize": Nl * (32 + 8)}
     dom = max(alg, key=lambda k: stages[k])
+    # DRAM bytes (read + write) per unit from one ncu capture of each kernel on
+    # the csg1m workload (profiles/occupancy_kernels_csg1m.md), scaled by the
+    # units of this run: links for the cone passes, leaves for the priors
+    units = {"occ.sampleness": n * K, "occ.emptiness": n * K, "occ.priors": Nl}
+    traffic = None
+    if dom in TRAFFIC_PER_UNIT:
+        traffic = int(TRAFFIC_PER_UNIT[dom] * units[dom])
     hbm, src = peaks()
     achieved = alg[dom] / (stages[dom] / 1e3) / 1e9
     total_ms = sum(v for k, v in stages.items() if not k.startswith("sub."))
@@ -318,13 +346,17 @@ def our_arm(args):
                    "sampling": {"rounds": tc.sampling_rounds, "waves": tc.sampling_waves,
                                 "writers": tc.sampling_writers}},
         "e2e": None if t_e2e is None else {"value": world_samples * args.steps / t_e2e, "unit": UNIT,
-                                            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+                                            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                                            "step_ms": [round(x, 3) for x in e2e_step_ms]},
         "gpu_launches": int(launches),
+        "step_ms": [round(x, 3) for x in step_ms],
         "stage_ms": {k: round(v, 3) for k, v in stages.items()},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm,
                      "unit": "GB/s", "frac": achieved / hbm, "peak_source": src + " (MEASURED_PEAKS.json hbm_gbs)",
                      "algorithmic_bytes": int(alg[dom]), "kernel_ms": stages[dom],
-                     "share_of_step": stages[dom] / total_ms if total_ms else None, "traffic": None},
+                     "share_of_step": stages[dom] / total_ms if total_ms else None, "traffic": traffic,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per unit on csg1m, "
+                                       "scaled to this run's units"},
         "clocks": clk,
     }
     if rank == 0 and not args.no_cpu_baseline:
