@@ -168,7 +168,7 @@ TSR_API tsr_status tsr_tree_copy_leaves(const tsr_tree *tree, double *scopes, ui
                                 uint32_t *neighbors);
 TSR_API tsr_status tsr_tree_copy_dual_cells(const tsr_tree *tree, uint32_t *cells8);
 
-/* mode 0 = plain FP32 field with compensated per-leaf sums. */
+/* mode 0 = plain field: FP32 kernel values, FP64 per-leaf sums. */
 TSR_API tsr_status tsr_occupancy_compute(const tsr_tree *tree, const tsr_cameras_view *cameras,
                                  const tsr_params *params, int mode, void *cuda_stream,
                                  tsr_occupancy **out_occupancy);

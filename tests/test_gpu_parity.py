@@ -2,7 +2,7 @@
 
 Bit-exact: root scope, node arrays, sample permutation, leaf scopes, node->leaf
 links, neighbour CSR, dual-cell list, and the DMC mesh computed from the same
-field.  Tolerance (FP32 field with compensated sums vs the FP64 oracle):
+field.  Tolerance (FP32 kernel values with FP64 sums vs the FP64 oracle):
 stated per field below.
 """
 import numpy as np

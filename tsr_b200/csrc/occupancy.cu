@@ -9,13 +9,11 @@
 //
 // Precision: the per-link cone set-up, the depth cap, the cone length and the
 // cone count are FP64 (as the reference's Real = double); kernel evaluation
-// runs in FP32 in a frame centred on the sample, and every per-leaf sum is a
-// compensated FP32 pair (sum, rounding error): each atomic add returns the
-// old sum, the exact rounding error of that add (Knuth's TwoSum) goes into
-// the second word.  Priors and occupancy are evaluated in FP64 from the
-// compensated sums; the prior's sphere / box membership test is the same FP64
-// expression as the tree build's, so the set of leaves each prior sums over
-// is exact.
+// runs in FP32 in a frame centred on the sample, and every per-leaf sum is an
+// FP64 accumulator updated by FP64 atomic adds whose result is not used (no
+// round trip per accepted pair).  Priors and occupancy are evaluated in FP64;
+// the prior's sphere / box membership test is the same FP64 expression as the
+// tree build's, so the set of leaves each prior sums over is exact.
 #include <cub/cub.cuh>
 
 #include <vector>
