@@ -104,7 +104,28 @@ typedef struct {
     uint64_t visited_sampleness;       /* tree nodes tested against a cone, SAMPLENESS pass */
     uint64_t visited_emptiness;        /* ... EMPTINESS pass */
     uint64_t visited_priors;           /* tree nodes classified by the prior sphere queries */
+    uint64_t pruned_leaves;            /* leaves the learned pruner skipped (0 for the plain field) */
 } tsr_occupancy_counts;
+
+/* The learned pruner (north_star's MLP; no counterpart in the reference).
+ * A 10 -> 64 -> 64 -> 2 ReLU MLP over per-leaf features (tsr_occupancy_leaf_features)
+ * with two logits: "occupancy > 0" and "near a sign change".  Parameters are
+ * FP32, TSR_MLP_PARAMS values in the order W1[10][64], b1[64], W2[64][64],
+ * b2[64], W3[64][2], b3[2] (W[in][out]). */
+#define TSR_MLP_FEATURES 10
+#define TSR_MLP_HIDDEN 64
+#define TSR_MLP_OUTPUTS 2
+#define TSR_MLP_PARAMS 4994
+
+typedef struct {
+    const float *weights;              /* HOST, TSR_MLP_PARAMS values */
+    float feature_mean[TSR_MLP_FEATURES];
+    float feature_inv_std[TSR_MLP_FEATURES];   /* inputs are (feature - mean) * inv_std */
+    float sign_threshold;              /* the sign is taken as known when P(occupancy > 0) is below this
+                                          or above 1 - this (0 < sign_threshold < 0.5) */
+    float band_threshold;              /* a leaf counts as near a sign change when P(band) >= this */
+    uint32_t dilation;                 /* rings of face neighbours added around those leaves */
+} tsr_pruner;
 
 typedef struct tsr_tree tsr_tree;
 typedef struct tsr_occupancy tsr_occupancy;
@@ -187,6 +208,42 @@ TSR_API tsr_status tsr_mesh_get_counts(const tsr_mesh *mesh, tsr_mesh_counts *ou
  * uint32 per triangle.  Any pointer may be NULL. */
 TSR_API tsr_status tsr_mesh_copy(const tsr_mesh *mesh, uint8_t *cases, double *positions, double *scales,
                          uint32_t *edge_keys, uint32_t *triangles);
+
+/* ---- learned pruner (no counterpart in the reference) ---- */
+/* The pruner's per-leaf features of a field, leaves x TSR_MLP_FEATURES floats
+ * into HOST memory: log1p(samples in the leaf), log(mean sample scale / leaf
+ * size), normal spread (1 - |mean normal|), depth / 16, log1p(E), log1p(S),
+ * r = S / (E + S) (-1 when both are 0), reliable (E + S >= threshold) as 0/1,
+ * and the smallest and largest r among the face neighbours.  Everything is
+ * known before the prior queries. */
+TSR_API tsr_status tsr_occupancy_leaf_features(const tsr_tree *tree, const tsr_occupancy *occ, float *features);
+/* Training on DEVICE arrays: x (n x 10, normalized), y (n x 2 labels in
+ * {0,1}), params (TSR_MLP_PARAMS).  Adds the gradient of the summed
+ * binary cross-entropy (positive labels of output k weighted by
+ * pos_weight[k]) to grads and the summed loss to *loss (both device). */
+TSR_API tsr_status tsr_mlp_train_batch(const float *x, const float *y, uint32_t n, const float *params,
+                                       float *grads, float *loss, float pos_weight0, float pos_weight1,
+                                       void *cuda_stream);
+/* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8) on DEVICE arrays; the
+ * gradient is multiplied by grad_scale first; step counts from 1. */
+TSR_API tsr_status tsr_mlp_adam(float *params, const float *grads, float *m, float *v, uint32_t step,
+                                float lr, float grad_scale, void *cuda_stream);
+/* Logits (n x 2, DEVICE) of normalized DEVICE features: FP32 reference, and
+ * the BF16 tensor-core path (mma.sync, FP32 accumulation) the pruner uses. */
+TSR_API tsr_status tsr_mlp_forward(const float *x, uint32_t n, const float *params, float *logits,
+                                   void *cuda_stream);
+TSR_API tsr_status tsr_mlp_infer_bf16(const float *x, uint32_t n, const float *params, float *logits,
+                                      void *cuda_stream);
+/* The pruned field: like tsr_occupancy_compute (both cone passes exact), but
+ * the prior query -- the most expensive per-leaf step -- runs only for
+ * reliable leaves (E + S >= confidenceThreshold) that the pruner places near
+ * a sign change (or within `dilation` rings of face neighbours of one) or
+ * whose sign it is not sure of; E == 0 or S == 0 fixes the sign without a
+ * prior.  A skipped reliable leaf takes the pruner's sign, with the value
+ * 0.5 (S - E) / coneCount when positive; its prior reads NaN. */
+TSR_API tsr_status tsr_occupancy_compute_pruned(const tsr_tree *tree, const tsr_cameras_view *cameras,
+                                                const tsr_params *params, const tsr_pruner *pruner,
+                                                void *cuda_stream, tsr_occupancy **out_occupancy);
 
 /* Number of this library's kernel launches so far in the process
  * (instrumentation; no counterpart in the reference). */

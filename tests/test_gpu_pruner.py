@@ -1,0 +1,50 @@
+"""The pruned field with the committed trained network, judged by the plain
+method on a scene the network never saw (random CSG scene, seed 500).
+
+What the network gains over the method without it: the prior queries of
+the leaves it places away from a sign change are skipped (fewer tree nodes
+classified), while the mesh stays the plain method's."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+MIN_CASE_AGREEMENT = 0.999        # DMC case codes equal to the plain field's
+MAX_HAUSDORFF_LEAVES = 0.1        # vertex Hausdorff distance, in finest leaf sizes
+MIN_PRIOR_WORK_SAVED = 0.25       # fraction of prior-query node visits removed
+
+
+@pytest.fixture(scope="module")
+def heldout():
+    from tsr_b200 import core, scenes
+    sc = scenes.random_csg_scene(seed=500, n_target=200_000, width=480, height=360, f=400.0)
+    tree = core.Tree(core.Samples.from_scene(sc), reorder_samples=False)
+    return tree, core.Cameras(sc.cams)
+
+
+def test_pruned_field_matches_plain_mesh_with_less_work(heldout):
+    from tsr_b200 import core, pruner
+    tree, cams = heldout
+    j = pruner.judge(tree, cams, core.Pruner.load())
+    saved = 1.0 - j["visited"]["visited_priors"][1] / j["visited"]["visited_priors"][0]
+    assert j["case_agreement"] >= MIN_CASE_AGREEMENT, j
+    assert j["vertex_hausdorff"] <= MAX_HAUSDORFF_LEAVES * j["finest_leaf_size"], j
+    assert saved >= MIN_PRIOR_WORK_SAVED, j
+    # the cone passes are not pruned: same work as the plain field
+    assert j["visited"]["visited_sampleness"][0] == j["visited"]["visited_sampleness"][1]
+
+
+def test_pruned_field_keeps_exact_values_where_queried(heldout):
+    from tsr_b200 import core
+    tree, cams = heldout
+    plain = core.Occupancy(tree, cams)
+    pruned = core.Occupancy(tree, cams, pruner=core.Pruner.load())
+    pp, pq = plain.getPriorForEmptiness(), pruned.getPriorForEmptiness()
+    queried = ~np.isnan(pq)
+    assert queried.sum() > 0 and (~queried).sum() == pruned.counts["pruned_leaves"]
+    np.testing.assert_allclose(pq[queried], pp[queried], rtol=0, atol=1e-12)
+    oq, op = pruned.getOccupancy(), plain.getOccupancy()
+    # the FP64 atomic sums may round differently from run to run
+    np.testing.assert_allclose(oq[queried], op[queried], rtol=1e-9, atol=1e-15)
+    # the cone passes are the plain field's in the pruned field
+    np.testing.assert_allclose(pruned.field("emptiness_sum"), plain.field("emptiness_sum"), rtol=1e-12, atol=0)

@@ -59,7 +59,17 @@ class tsr_mesh_counts(ctypes.Structure):
 
 class tsr_occupancy_counts(ctypes.Structure):
     _fields_ = [("links", _U64), ("accepted_sampleness", _U64), ("accepted_emptiness", _U64),
-                ("visited_sampleness", _U64), ("visited_emptiness", _U64), ("visited_priors", _U64)]
+                ("visited_sampleness", _U64), ("visited_emptiness", _U64), ("visited_priors", _U64),
+                ("pruned_leaves", _U64)]
+
+
+MLP_FEATURES, MLP_HIDDEN, MLP_OUTPUTS, MLP_PARAMS = 10, 64, 2, 4994
+
+
+class tsr_pruner(ctypes.Structure):
+    _fields_ = [("weights", _P), ("feature_mean", ctypes.c_float * MLP_FEATURES),
+                ("feature_inv_std", ctypes.c_float * MLP_FEATURES), ("sign_threshold", ctypes.c_float),
+                ("band_threshold", ctypes.c_float), ("dilation", _U32)]
 
 
 lib = ctypes.CDLL(str(_LIB_PATH))
@@ -89,6 +99,13 @@ _sig = {
     "tsr_mesh_free": (None, [_P]),
     "tsr_mesh_get_counts": (ctypes.c_int, [_P, _P]),
     "tsr_mesh_copy": (ctypes.c_int, [_P, _P, _P, _P, _P, _P]),
+    "tsr_occupancy_leaf_features": (ctypes.c_int, [_P, _P, _P]),
+    "tsr_mlp_train_batch": (ctypes.c_int, [_P, _P, ctypes.c_uint32, _P, _P, _P, ctypes.c_float, ctypes.c_float,
+                                           _P]),
+    "tsr_mlp_adam": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_uint32, ctypes.c_float, ctypes.c_float, _P]),
+    "tsr_mlp_forward": (ctypes.c_int, [_P, ctypes.c_uint32, _P, _P, _P]),
+    "tsr_mlp_infer_bf16": (ctypes.c_int, [_P, ctypes.c_uint32, _P, _P, _P]),
+    "tsr_occupancy_compute_pruned": (ctypes.c_int, [_P, _P, _P, _P, _P, _P]),
 }
 for _name, (_res, _args) in _sig.items():
     _f = getattr(lib, _name)
@@ -335,12 +352,22 @@ class Occupancy:
 
     EMPTINESS, SAMPLENESS = 0, 1
 
-    def __init__(self, tree: Tree, cameras: Cameras, params=None, mode=0, stream=None):
+    def __init__(self, tree: Tree, cameras: Cameras, params=None, mode=0, stream=None, pruner=None):
+        """pruner: a ``Pruner`` -- the pruned field (no counterpart in the
+        reference); None computes the plain field like the reference."""
         self._h = _P()
         self.tree = tree
         p = params or tree.params
-        _check(lib.tsr_occupancy_compute(tree.handle, ctypes.byref(cameras.view()), ctypes.byref(p), mode,
-                                         _stream_ptr(stream), ctypes.byref(self._h)))
+        if pruner is None:
+            _check(lib.tsr_occupancy_compute(tree.handle, ctypes.byref(cameras.view()), ctypes.byref(p), mode,
+                                             _stream_ptr(stream), ctypes.byref(self._h)))
+        else:
+            pv = pruner.view()
+            _check(lib.tsr_occupancy_compute_pruned(tree.handle, ctypes.byref(cameras.view()), ctypes.byref(p),
+                                                    ctypes.byref(pv), _stream_ptr(stream), ctypes.byref(self._h)))
+        c = tsr_occupancy_counts()
+        _check(lib.tsr_occupancy_get_counts(self._h, ctypes.byref(c)))
+        self.counts = {k: int(getattr(c, k)) for k, _ in tsr_occupancy_counts._fields_}
         self._cache = {}
         self.mCrust = None
         self._stream = stream
@@ -353,6 +380,19 @@ class Occupancy:
     @property
     def handle(self):
         return self._h
+
+    def getLeafFeatures(self):
+        """The learned pruner's per-leaf features (leaves x 10 float32)."""
+        f = np.zeros((self.tree.counts["leaves"], MLP_FEATURES), np.float32)
+        _check(lib.tsr_occupancy_leaf_features(self.tree.handle, self._h, _ptr(f)))
+        return f
+
+    def stage_ms(self):
+        """CUDA-event milliseconds of the field's stages."""
+        ms = np.zeros(8, np.float32)
+        _check(lib.tsr_occupancy_stage_ms(self._h, _ptr(ms), 8))
+        names = ["sampleness", "flags", "emptiness", "priors", "finalize"]
+        return {k: float(v) for k, v in zip(names, ms)}
 
     def field(self, name):
         if name not in self._cache:
@@ -426,6 +466,47 @@ class DualMarchingCells:
 
     def getSurface(self):
         return self.positions, self.triangles
+
+
+class Pruner:
+    """The learned pruner's network and decision thresholds (new; no
+    counterpart in the reference).  ``weights``: TSR_MLP_PARAMS float32 values
+    (W1[10][64], b1, W2[64][64], b2, W3[64][2], b3); features are normalized
+    as (f - mean) * inv_std."""
+
+    def __init__(self, weights, mean, inv_std, sign_threshold, band_threshold, dilation=1):
+        self.weights = np.ascontiguousarray(weights, np.float32).reshape(-1)
+        if self.weights.shape[0] != MLP_PARAMS:
+            raise ValueError("expected %d weights" % MLP_PARAMS)
+        self.mean = np.asarray(mean, np.float32).reshape(MLP_FEATURES)
+        self.inv_std = np.asarray(inv_std, np.float32).reshape(MLP_FEATURES)
+        self.sign_threshold = float(sign_threshold)
+        self.band_threshold = float(band_threshold)
+        self.dilation = int(dilation)
+
+    @classmethod
+    def load(cls, path=None):
+        path = Path(path) if path else Path(__file__).resolve().parent / "pruner_weights.npz"
+        z = np.load(path)
+        return cls(z["weights"], z["mean"], z["inv_std"], float(z["sign_threshold"]), float(z["band_threshold"]),
+                   int(z["dilation"]))
+
+    def save(self, path, **extra):
+        np.savez(path, weights=self.weights, mean=self.mean, inv_std=self.inv_std,
+                 sign_threshold=np.float32(self.sign_threshold), band_threshold=np.float32(self.band_threshold),
+                 dilation=np.int32(self.dilation), **extra)
+
+    def view(self):
+        v = tsr_pruner()
+        v.weights = self.weights.ctypes.data_as(_P)
+        for i in range(MLP_FEATURES):
+            v.feature_mean[i] = float(self.mean[i])
+            v.feature_inv_std[i] = float(self.inv_std[i])
+        v.sign_threshold = self.sign_threshold
+        v.band_threshold = self.band_threshold
+        v.dilation = self.dilation
+        self._keep = self.weights   # the C side reads the weights during the call
+        return v
 
 
 def version():

@@ -278,6 +278,80 @@ tsr_status tsr_occupancy_compute(const tsr_tree *tree, const tsr_cameras_view *c
     });
 }
 
+tsr_status tsr_occupancy_compute_pruned(const tsr_tree *tree, const tsr_cameras_view *cameras,
+                                        const tsr_params *params, const tsr_pruner *pruner, void *cuda_stream,
+                                        tsr_occupancy **out) {
+    if (out) *out = nullptr;
+    return guarded([&] {
+        if (!tree || !cameras || !out || !pruner) fail(TSR_ERR_INVALID_ARG, "null argument");
+        if (!pruner->weights) fail(TSR_ERR_INVALID_ARG, "null pruner weights");
+        if (!(pruner->sign_threshold > 0.0f && pruner->sign_threshold < 0.5f) ||
+            !(pruner->band_threshold > 0.0f && pruner->band_threshold < 1.0f))
+            fail(TSR_ERR_INVALID_ARG, "pruner thresholds: sign in (0, 0.5), band in (0, 1)");
+        if (pruner->dilation > 64) fail(TSR_ERR_INVALID_ARG, "pruner dilation above 64 rings");
+        if (cameras->count && !cameras->positions) fail(TSR_ERR_INVALID_ARG, "null camera positions");
+        if (tree->n_leaves == 0) fail(TSR_ERR_STATE, "tree has no leaves");
+        tsr_params p = tree->params;
+        if (params) p = *params;
+        check_params(p);
+        if (p.max_relative_sampling_distance != tree->params.max_relative_sampling_distance)
+            fail(TSR_ERR_INVALID_ARG, "h_SVO must match the tree's");
+        tsr_occupancy *o = new tsr_occupancy();
+        o->stream = (cudaStream_t)cuda_stream;
+        try {
+            compute_occupancy(*tree, *cameras, p, 0, *o, pruner);
+        } catch (...) {
+            delete o;
+            throw;
+        }
+        *out = o;
+    });
+}
+
+tsr_status tsr_occupancy_leaf_features(const tsr_tree *t, const tsr_occupancy *o, float *features) {
+    return guarded([&] {
+        if (!t || !o || !features) fail(TSR_ERR_INVALID_ARG, "null argument");
+        if (o->n_leaves != t->n_leaves) fail(TSR_ERR_INVALID_ARG, "field of another tree");
+        DBuf<float> f;
+        leaf_features(*t, o->e_sum.p, o->s_sum.p, o->confidence_threshold, f, o->stream);
+        TSR_CUDA(cudaMemcpyAsync(features, f.p, (size_t)t->n_leaves * TSR_MLP_FEATURES * sizeof(float),
+                                 cudaMemcpyDeviceToHost, o->stream));
+        TSR_CUDA(cudaStreamSynchronize(o->stream));
+    });
+}
+
+tsr_status tsr_mlp_train_batch(const float *x, const float *y, uint32_t n, const float *params, float *grads,
+                               float *loss, float pos_weight0, float pos_weight1, void *cuda_stream) {
+    return guarded([&] {
+        if (!x || !y || !params || !grads || !loss) fail(TSR_ERR_INVALID_ARG, "null argument");
+        mlp_train_batch(x, y, n, params, grads, loss, pos_weight0, pos_weight1, (cudaStream_t)cuda_stream);
+    });
+}
+
+tsr_status tsr_mlp_adam(float *params, const float *grads, float *m, float *v, uint32_t step, float lr,
+                        float grad_scale, void *cuda_stream) {
+    return guarded([&] {
+        if (!params || !grads || !m || !v) fail(TSR_ERR_INVALID_ARG, "null argument");
+        if (step == 0) fail(TSR_ERR_INVALID_ARG, "Adam steps count from 1");
+        mlp_adam(params, grads, m, v, step, lr, grad_scale, (cudaStream_t)cuda_stream);
+    });
+}
+
+tsr_status tsr_mlp_forward(const float *x, uint32_t n, const float *params, float *logits, void *cuda_stream) {
+    return guarded([&] {
+        if (!x || !params || !logits) fail(TSR_ERR_INVALID_ARG, "null argument");
+        mlp_forward(x, n, params, logits, (cudaStream_t)cuda_stream);
+    });
+}
+
+tsr_status tsr_mlp_infer_bf16(const float *x, uint32_t n, const float *params, float *logits,
+                              void *cuda_stream) {
+    return guarded([&] {
+        if (!x || !params || !logits) fail(TSR_ERR_INVALID_ARG, "null argument");
+        mlp_infer_bf16(x, n, params, logits, (cudaStream_t)cuda_stream);
+    });
+}
+
 void tsr_occupancy_free(tsr_occupancy *o) { delete o; }
 
 tsr_status tsr_occupancy_get_counts(const tsr_occupancy *o, tsr_occupancy_counts *out) {
@@ -289,6 +363,7 @@ tsr_status tsr_occupancy_get_counts(const tsr_occupancy *o, tsr_occupancy_counts
         out->visited_sampleness = o->visits[1];
         out->visited_emptiness = o->visits[0];
         out->visited_priors = o->visits[2];
+        out->pruned_leaves = o->pruned;
     });
 }
 

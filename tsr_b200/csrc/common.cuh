@@ -21,6 +21,9 @@ constexpr double REAL_MAX = 1.7976931348623157e308;
 constexpr uint32_t MAX_DEPTH_DIFFERENCE = 3;       // Occupancy.cpp:72
 constexpr uint32_t FLAG_SAMPLENESS = 1u;           // Occupancy.h:38
 constexpr uint32_t FLAG_EMPTINESS = 2u;            // Occupancy.h:39
+// per-leaf predictions of the learned pruner: near a sign change (or within
+// the dilation ring), confidently positive, confidently not positive
+constexpr uint8_t PRED_KEEP = 1, PRED_POS = 2, PRED_NEG = 4;
 constexpr int MAX_TREE_DEPTH = 40;                 // stack bound of the traversals
 
 struct Error {

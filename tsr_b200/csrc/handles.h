@@ -41,10 +41,12 @@ struct tsr_occupancy {
     tsr::DBuf<double> e_sum, s_sum, e_len, s_len, prior, occ;
     tsr::DBuf<uint32_t> states;
     double cone_count = 0;
+    double confidence_threshold = 0;   // Occupancy::confidenceThreshold of this field
     float stage_ms[8] = {0};
     uint64_t accepted[2] = {0, 0};   // [EMPTINESS, SAMPLENESS]
     uint64_t visits[3] = {0, 0, 0};  // nodes tested: EMPTINESS, SAMPLENESS, priors
     uint64_t links = 0;
+    uint64_t pruned = 0;             // leaves whose prior query the pruned field skipped
 };
 
 struct tsr_mesh {
@@ -58,7 +60,17 @@ struct tsr_mesh {
 namespace tsr {
 void build_tree(tsr_tree &t, const tsr_samples_view &sv, bool on_device);
 void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_params &p, int mode,
-                       tsr_occupancy &o);
+                       tsr_occupancy &o, const tsr_pruner *pruner = nullptr);
+void leaf_features(const tsr_tree &t, const double *esum, const double *ssum, double threshold, DBuf<float> &feat,
+                   cudaStream_t st);
+void mlp_train_batch(const float *x, const float *y, uint32_t n, const float *params, float *grads, float *loss,
+                     float pw0, float pw1, cudaStream_t st);
+void mlp_adam(float *p, const float *g, float *m, float *v, uint32_t step, float lr, float gscale,
+              cudaStream_t st);
+void mlp_forward(const float *x, uint32_t n, const float *params, float *out, cudaStream_t st);
+void mlp_infer_bf16(const float *x, uint32_t n, const float *params, float *out, cudaStream_t st);
+void pruner_predict(const tsr_tree &t, const tsr_pruner &pr, const double *esum, const double *ssum,
+                    double threshold, DBuf<uint8_t> &pred, cudaStream_t st);
 void extract_dmc(const tsr_tree &t, const tsr_occupancy &o, tsr_mesh &m);
 void root_scope_noalloc(uint64_t count, const double *positions, const double *scales, double h_svo,
                         double *out_min_xyz_size, cudaStream_t st);

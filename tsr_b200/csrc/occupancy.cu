@@ -173,6 +173,25 @@ __global__ void k_pack_rec(uint32_t nn, const uint32_t *children, const uint32_t
     rec[i + REC_OFFSET] = make_uint2(c, y);
 }
 
+// Pruned field: which leaves need their prior.  Only a reliable leaf
+// (E + S >= confidenceThreshold) uses it, and with E == 0 or S == 0 its sign
+// is fixed without it; of the rest, the pruner lets a leaf skip the query
+// when it is neither near a predicted sign change (PRED_KEEP) nor of
+// uncertain sign (PRED_POS / PRED_NEG clear).
+__global__ void k_prior_needed(uint32_t nl, const uint8_t *pred, const double *esum, const double *ssum,
+                               double threshold, uint8_t *need) {
+    uint32_t l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= nl) return;
+    const double e = esum[l], s = ssum[l];
+    const uint8_t pr = pred[l];
+    bool n = false;
+    if (!((e + s) < threshold)) {
+        if (pr & PRED_KEEP) n = true;
+        else if (e > 0.0 && s > 0.0 && !(pr & (PRED_POS | PRED_NEG))) n = true;
+    }
+    need[l] = n ? 1 : 0;
+}
+
 __device__ __forceinline__ F3 child_min(F3 pmin, uint32_t ci, float size) {
     return f3((ci & 1u) ? pmin.x + size : pmin.x, (ci & 2u) ? pmin.y + size : pmin.y,
               (ci & 4u) ? pmin.z + size : pmin.z);
@@ -469,6 +488,11 @@ __global__ void __launch_bounds__(PT_BLOCK, (TYPE == 0) ? 6 : 5) k_cone_x(uint64
     }
 }
 
+__global__ void k_iota(uint32_t n, uint32_t *out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = i;
+}
+
 // A leaf carries a type's flag exactly when it received a kernel of that type.
 __global__ void k_leaf_flags(uint32_t nl, const uint32_t *leaf_node, const double *ksum, uint32_t *states,
                              uint32_t flag) {
@@ -568,7 +592,8 @@ __device__ inline bool box_inside_sphere(const D3 &mn, double sz, const D3 &c, d
 // 64-byte line and their FP64 boxes are derived from the parent's corner with
 // the tree build's own recurrence (child_coords, exact), so no node geometry
 // is loaded inside the loop.
-__global__ void __launch_bounds__(PT_BLOCK) k_priors_x(uint32_t nl, uint32_t nn, const uint32_t *leaf_node, const D3 *leaf_min,
+__global__ void __launch_bounds__(PT_BLOCK) k_priors_x(uint32_t nl, uint32_t nn, const uint32_t *list,
+                                                      const uint32_t *leaf_node, const D3 *leaf_min,
                                                       const uint8_t *depth, const D3 *nmin, const uint2 *rec,
                                                       const double2 *psum, double root_size, double rel_radius,
                                                       double *prior, unsigned long long *next_leaf,
@@ -617,7 +642,7 @@ __global__ void __launch_bounds__(PT_BLOCK) k_priors_x(uint32_t nl, uint32_t nn,
                 if (i >= nl) {
                     done = true;
                 } else {
-                    l = (uint32_t)i;
+                    l = list ? list[i] : (uint32_t)i;
                     uint32_t node = leaf_node[l];
                     uint32_t ld = depth[node];
                     double size = size_at(root_size, ld);
@@ -704,9 +729,15 @@ __global__ void __launch_bounds__(PT_BLOCK) k_priors_x(uint32_t nl, uint32_t nn,
 }
 
 // Occupancy::getOccupancy (Occupancy.cpp:570-587), FP64.
+// Occupancy::getOccupancy (Occupancy.cpp:570-587), FP64.  In a pruned field
+// (pred != null) a reliable leaf whose prior was not queried (need == 0)
+// gets its sign from E == 0 / S == 0 or from the pruner, and the value
+// 0.5 (S - E) / coneCount for a positive sign (the value at prior 1/2), so
+// only leaves away from a predicted sign change carry an approximate value.
 __global__ void k_finalize(uint32_t nl, const double *esum, const double *ssum, const double *elen,
                            const double *slen, const double *prior, double cone_count, double threshold,
-                           double *o_esum, double *o_ssum, double *o_elen, double *o_slen, double *occ) {
+                           const uint8_t *pred, const uint8_t *need, double *o_esum, double *o_ssum,
+                           double *o_elen, double *o_slen, double *occ) {
     uint32_t l = blockIdx.x * blockDim.x + threadIdx.x;
     if (l >= nl) return;
     double e = esum[l], s = ssum[l];
@@ -717,6 +748,10 @@ __global__ void k_finalize(uint32_t nl, const double *esum, const double *ssum, 
     double v;
     if ((e + s) < threshold) {
         v = -EPS;
+    } else if (pred && !need[l]) {
+        const bool pos = (e == 0.0) ? true : (s == 0.0) ? false : (pred[l] & PRED_POS) != 0;
+        const double approx = 0.5 * (s - e) / cone_count;
+        v = (pos && approx > 0.0) ? approx : (pos ? EPS : -EPS);
     } else {
         double pr = prior[l];
         double pe = pr * (e / cone_count);
@@ -748,12 +783,13 @@ struct Timer {
 }  // namespace
 
 void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_params &p, int mode,
-                       tsr_occupancy &o) {
+                       tsr_occupancy &o, const tsr_pruner *pruner) {
     (void)mode;
     cudaStream_t st = o.stream;
     const uint32_t nl = t.n_leaves, nn = t.n_nodes;
     o.n_leaves = nl;
     o.n_nodes = nn;
+    o.confidence_threshold = p.confidence_threshold;
     Timer timer(st);
     DBuf<D3> cams(cv.count, st);
     if (cv.count) TSR_CUDA(cudaMemcpyAsync(cams.p, cv.positions, (size_t)cv.count * 24, cudaMemcpyHostToDevice, st));
@@ -818,7 +854,8 @@ void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_
         k_forward_flag<<<grid_for(hi - lo, BLK), BLK, 0, st>>>(lo, hi, t.level_order.p, t.children.p, o.states.p,
                                                               FLAG_SAMPLENESS); ::tsr::note_launch();
     }
-    k_pack_rec<<<grid_for(nn, BLK), BLK, 0, st>>>(nn, t.children.p, t.node_to_leaf.p, o.states.p, recs.p); ::tsr::note_launch();
+    k_pack_rec<<<grid_for(nn, BLK), BLK, 0, st>>>(nn, t.children.p, t.node_to_leaf.p, o.states.p, recs.p);
+    ::tsr::note_launch();
     o.stage_ms[1] = timer.lap();
     next_link.zero();
     k_link_setup<EMPTINESS><<<grid_for(nlinks, 128), 128, 0, st>>>(nlinks, order.p, in, tr, recs.p, lrec.p, esum,
@@ -830,7 +867,31 @@ void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_
     k_leaf_flags<<<grid_for(nl, BLK), BLK, 0, st>>>(nl, t.leaf_node.p, esum, o.states.p, FLAG_EMPTINESS); ::tsr::note_launch();
     o.stage_ms[2] = timer.lap();
     o.prior.alloc(nl, st);
+    DBuf<uint8_t> need;   // pruned field: leaves whose prior is queried
+    DBuf<uint8_t> pred_buf;
+    if (pruner) pruner_predict(t, *pruner, esum, ssum, p.confidence_threshold, pred_buf, st);
+    const uint8_t *pred = pred_buf.p;
+    if (pred) {
+        o.prior.fill_bytes(0xFF);   // NaN: no prior where the query was skipped
+        need.alloc(nl, st);
+        k_prior_needed<<<grid_for(nl, BLK), BLK, 0, st>>>(nl, pred, esum, ssum, p.confidence_threshold, need.p);
+        ::tsr::note_launch();
+    }
     {
+        // the queried leaves: all of them, or the selected ones of a pruned field
+        DBuf<uint32_t> list;
+        uint32_t nq = nl;
+        if (pred) {
+            DBuf<uint32_t> ids(nl, st), nsel(1, st);
+            list.alloc(nl, st);
+            k_iota<<<grid_for(nl, BLK), BLK, 0, st>>>(nl, ids.p); ::tsr::note_launch();
+            size_t tmp = 0;
+            TSR_CUDA(cub::DeviceSelect::Flagged(nullptr, tmp, ids.p, need.p, list.p, nsel.p, (int)nl, st));
+            DBuf<uint8_t> tb(tmp, st);
+            TSR_CUDA(cub::DeviceSelect::Flagged(tb.p, tmp, ids.p, need.p, list.p, nsel.p, (int)nl, st));
+            nq = read_scalar(nsel.p, st);
+            o.pruned = nl - nq;
+        }
         DBuf<double2> psum((size_t)nn * PK, st);
         for (int d = (int)t.level_start.size() - 2; d >= 0; --d) {
             uint32_t lo = t.level_start[d], hi = t.level_start[d + 1];
@@ -838,7 +899,7 @@ void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_
                                                                 t.node_to_leaf.p, o.states.p, elen, slen, psum.p); ::tsr::note_launch();
         }
         next_link.zero();
-        k_priors_x<<<prior_grid, PT_BLOCK, 0, st>>>(nl, nn, t.leaf_node.p, t.leaf_min.p, t.depth.p, t.nmin.p, recs.p,
+        k_priors_x<<<prior_grid, PT_BLOCK, 0, st>>>(nq, nn, list.p, t.leaf_node.p, t.leaf_min.p, t.depth.p, t.nmin.p, recs.p,
                                                    psum.p, t.root_size, p.relative_radius_for_priors, o.prior.p,
                                                    next_link.p, accepted.p + 4, err.p);
         ::tsr::note_launch();
@@ -847,8 +908,8 @@ void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_
     o.cone_count = read_scalar(cone_count.p, st);
     o.e_sum.alloc(nl, st); o.s_sum.alloc(nl, st); o.e_len.alloc(nl, st); o.s_len.alloc(nl, st); o.occ.alloc(nl, st);
     k_finalize<<<grid_for(nl, BLK), BLK, 0, st>>>(nl, esum, ssum, elen, slen, o.prior.p, o.cone_count,
-                                                 p.confidence_threshold, o.e_sum.p, o.s_sum.p, o.e_len.p, o.s_len.p,
-                                                 o.occ.p); ::tsr::note_launch();
+                                                 p.confidence_threshold, pred, need.p, o.e_sum.p, o.s_sum.p,
+                                                 o.e_len.p, o.s_len.p, o.occ.p); ::tsr::note_launch();
     o.stage_ms[4] = timer.lap();
     unsigned long long a[5];
     TSR_CUDA(cudaMemcpyAsync(a, accepted.p, sizeof(a), cudaMemcpyDeviceToHost, st));

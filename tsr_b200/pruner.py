@@ -1,0 +1,226 @@
+"""Training and evaluation of the learned pruner (new; no counterpart in the
+reference).
+
+The network (10 leaf features -> 64 -> 64 -> 2 logits) is trained on fields
+the plain method computes: label 0 is "occupancy > 0", label 1 is "near a
+sign change" (the leaf or one of its face neighbours has the other sign).
+Training runs on the GPU through the library's own kernels
+(tsr_mlp_train_batch: forward, backward and block-reduced gradients;
+tsr_mlp_adam); torch only provides device memory.  Two thresholds are
+chosen on a held-back scene: the band threshold misses at most ``miss`` of
+the leaves near a sign change, the sign threshold gives at most ``miss`` of
+the other leaves a confident but wrong sign.  The pruned field
+(tsr_occupancy_compute_pruned) skips the prior query of reliable leaves the
+network places away from a sign change (plus one ring of face neighbours)
+and whose sign it is sure of.
+
+    python -m tsr_b200.pruner --scenes 8 --samples 1000000 --out tsr_b200/pruner_weights.npz
+
+The committed ``pruner_weights.npz`` was produced by that command (its
+``meta`` entry records the arguments and the training statistics).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import time
+
+import numpy as np
+
+from . import core
+
+NF, NO = core.MLP_FEATURES, core.MLP_OUTPUTS
+
+
+def labels(occupancy, leaves):
+    """(sign, band) labels of every leaf from a plain field."""
+    s = np.asarray(occupancy) > 0.0
+    off = np.asarray(leaves.neighbors_offsets, np.int64)
+    nbs = np.asarray(leaves.neighbors, np.int64)
+    src = np.repeat(np.arange(s.shape[0]), np.diff(off))
+    diff = s[src] != s[nbs]
+    band = np.zeros(s.shape[0], bool)
+    band[src[diff]] = True
+    band[nbs[diff]] = True
+    return np.stack([s, band], 1).astype(np.float32)
+
+
+def scene_rows(scene, params=None):
+    """Features and labels of every leaf of one scene's plain field."""
+    samples = core.Samples.from_scene(scene)
+    tree = core.Tree(samples, params, reorder_samples=False)
+    occ = core.Occupancy(tree, core.Cameras(scene.cams), params)
+    return occ.getLeafFeatures(), labels(occ.getOccupancy(), tree.getLeaves())
+
+
+def he_init(seed=0):
+    rng = np.random.default_rng(seed)
+    parts = [rng.normal(0, np.sqrt(2.0 / NF), (NF, 64)), np.zeros(64), rng.normal(0, np.sqrt(2.0 / 64), (64, 64)),
+             np.zeros(64), rng.normal(0, np.sqrt(1.0 / 64), (64, NO)), np.zeros(NO)]
+    return np.concatenate([p.ravel() for p in parts]).astype(np.float32)
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _stream():
+    import torch
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def train(x, y, epochs=4, batch=8192, lr=3e-3, seed=0, pos_weight=None, log=None):
+    """Adam on normalized features x (rows x 10) and labels y (rows x 2);
+    returns the FP32 parameter vector."""
+    import torch
+    dev = torch.device("cuda")
+    n = x.shape[0]
+    if pos_weight is None:
+        frac = np.clip(y.mean(0), 1e-4, 0.5)
+        pos_weight = tuple(float(min(20.0, (1 - f) / f)) for f in frac)
+    xd = torch.from_numpy(np.ascontiguousarray(x, np.float32)).to(dev)
+    yd = torch.from_numpy(np.ascontiguousarray(y, np.float32)).to(dev)
+    theta = torch.from_numpy(he_init(seed)).to(dev)
+    grads = torch.zeros_like(theta)
+    m = torch.zeros_like(theta)
+    v = torch.zeros_like(theta)
+    loss = torch.zeros(1, dtype=torch.float32, device=dev)
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    step = 0
+    for ep in range(epochs):
+        perm = torch.randperm(n, generator=g).to(dev)
+        xs, ys = xd[perm].contiguous(), yd[perm].contiguous()
+        total = 0.0
+        loss.zero_()
+        for b0 in range(0, n, batch):
+            nb = min(batch, n - b0)
+            grads.zero_()
+            step += 1
+            core._check(core.lib.tsr_mlp_train_batch(_ptr(xs[b0:]), _ptr(ys[b0:]), nb, _ptr(theta), _ptr(grads),
+                                                     _ptr(loss), pos_weight[0], pos_weight[1], _stream()))
+            core._check(core.lib.tsr_mlp_adam(_ptr(theta), _ptr(grads), _ptr(m), _ptr(v), step,
+                                              lr * (0.5 ** (ep // 2)), 1.0 / nb, _stream()))
+        total = float(loss.item()) / n
+        if log:
+            log("epoch %d: mean weighted loss %.4f" % (ep, total))
+    return theta.cpu().numpy()
+
+
+def logits(theta, x, bf16=True):
+    """Logits of normalized features through the GPU kernels."""
+    import torch
+    dev = torch.device("cuda")
+    xd = torch.from_numpy(np.ascontiguousarray(x, np.float32)).to(dev)
+    th = torch.from_numpy(np.ascontiguousarray(theta, np.float32)).to(dev)
+    out = torch.empty((x.shape[0], NO), dtype=torch.float32, device=dev)
+    fn = core.lib.tsr_mlp_infer_bf16 if bf16 else core.lib.tsr_mlp_forward
+    core._check(fn(_ptr(xd), x.shape[0], _ptr(th), _ptr(out), _stream()))
+    return out.cpu().numpy()
+
+
+def choose_thresholds(z, y, miss=1e-3):
+    """(sign_threshold, band_threshold) from held-back rows: the band
+    threshold misses at most ``miss`` of the rows labelled near a sign change;
+    the sign threshold is the widest one for which at most ``miss`` of the
+    other rows get a confident but wrong sign."""
+    p = 1.0 / (1.0 + np.exp(-z.astype(np.float64)))
+    band = y[:, 1] > 0.5
+    tb = float(np.quantile(p[band, 1], miss)) if band.any() else 0.5
+    tb = min(max(tb, 1e-6), 0.999)
+    rest = ~band
+    ps, ys = p[rest, 0], y[rest, 0] > 0.5
+    ts = 1e-4
+    for cand in np.linspace(0.49, 1e-3, 250):
+        wrong = ((ps >= 1 - cand) & ~ys) | ((ps <= cand) & ys)
+        if wrong.mean() <= miss:
+            ts = float(cand)
+            break
+    return ts, tb
+
+
+def normalization(x):
+    mean = x.mean(0)
+    std = x.std(0)
+    return mean.astype(np.float32), (1.0 / np.maximum(std, 1e-6)).astype(np.float32)
+
+
+def fit(scenes, epochs=4, seed=0, miss=1e-3, dilation=1, log=print):
+    """Trains on the scenes' plain fields; the last scene is held back for
+    the threshold.  Returns a core.Pruner and a statistics dict."""
+    t0 = time.time()
+    rows = [scene_rows(s) for s in scenes]
+    x_tr = np.concatenate([r[0] for r in rows[:-1]])
+    y_tr = np.concatenate([r[1] for r in rows[:-1]])
+    x_va, y_va = rows[-1]
+    mean, istd = normalization(x_tr)
+    theta = train((x_tr - mean) * istd, y_tr, epochs=epochs, seed=seed, log=log)
+    z = logits(theta, (x_va - mean) * istd)
+    ts, tb = choose_thresholds(z, y_va, miss)
+    p = 1.0 / (1.0 + np.exp(-z.astype(np.float64)))
+    near = p[:, 1] >= tb
+    sure = (p[:, 0] >= 1 - ts) | (p[:, 0] <= ts)
+    band = y_va[:, 1] > 0.5
+    stats = {"train_rows": int(x_tr.shape[0]), "validation_rows": int(x_va.shape[0]),
+             "positive_fraction": float(y_tr[:, 0].mean()), "band_fraction": float(y_tr[:, 1].mean()),
+             "sign_threshold": ts, "band_threshold": tb,
+             "validation_predicted_band_fraction": float(near.mean()),
+             "validation_band_missed_fraction": float((band & ~near).sum() / max(1, band.sum())),
+             "validation_sure_sign_fraction": float(sure.mean()),
+             "seconds": time.time() - t0}
+    return core.Pruner(theta, mean, istd, ts, tb, dilation), stats
+
+
+def vertex_hausdorff(a, b):
+    """Symmetric Hausdorff distance between two vertex sets (an upper bound
+    of the vertex-to-surface distances of the two meshes)."""
+    from scipy.spatial import cKDTree
+    if len(a) == 0 or len(b) == 0:
+        return float("inf") if len(a) != len(b) else 0.0
+    return float(max(cKDTree(b).query(a)[0].max(), cKDTree(a).query(b)[0].max()))
+
+
+def judge(tree, cams, pruner, params=None, stream=None):
+    """The plain method judges the pruned field: both fields and meshes on
+    the same tree, with the pruned field's error and work savings."""
+    plain = core.Occupancy(tree, cams, params, stream=stream)
+    mesh_plain = plain.extractCrust()
+    pruned = core.Occupancy(tree, cams, params, stream=stream, pruner=pruner)
+    mesh_pruned = pruned.extractCrust()
+    op, oq = plain.getOccupancy(), pruned.getOccupancy()
+    scopes = tree.getLeaves().scopes
+    return {
+        "leaves": int(op.shape[0]),
+        "pruned_leaves": pruned.counts["pruned_leaves"],
+        "sign_agreement": float(np.mean((op > 0) == (oq > 0))),
+        "case_agreement": float(np.mean(mesh_plain.cases == mesh_pruned.cases)),
+        "triangles": [int(mesh_plain.triangles.shape[0]), int(mesh_pruned.triangles.shape[0])],
+        "vertex_hausdorff": vertex_hausdorff(mesh_plain.positions, mesh_pruned.positions),
+        "finest_leaf_size": float(scopes[:, 3].min()),
+        "visited": {k: [plain.counts[k], pruned.counts[k]] for k in
+                    ("visited_sampleness", "visited_emptiness", "visited_priors")},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    ap.add_argument("--scenes", type=int, default=8, help="random CSG scenes (the last one is held back)")
+    ap.add_argument("--samples", type=int, default=1_000_000)
+    ap.add_argument("--epochs", type=int, default=4)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--miss", type=float, default=1e-3)
+    ap.add_argument("--dilation", type=int, default=1)
+    ap.add_argument("--out", default="pruner_weights.npz")
+    a = ap.parse_args()
+    from . import scenes
+    t0 = time.time()
+    sc = [scenes.random_csg_scene(seed=1 + i, n_target=a.samples) for i in range(a.scenes)]
+    print("scenes generated in %.1f s" % (time.time() - t0), flush=True)
+    pruner, stats = fit(sc, epochs=a.epochs, seed=a.seed, miss=a.miss, dilation=a.dilation)
+    stats["args"] = vars(a)
+    print(json.dumps(stats), flush=True)
+    pruner.save(a.out, meta=np.array(json.dumps(stats)))
+
+
+if __name__ == "__main__":
+    main()
