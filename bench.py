@@ -207,13 +207,19 @@ def our_arm(args):
     dview = core.tsr_samples_view(n, scene.k, dev["pos"].data_ptr(), dev["nrm"].data_ptr(), dev["scale"].data_ptr(),
                                   dev["conf"].data_ptr(), dev["links"].data_ptr())
 
-    def device_step():
+    pruner_view = None
+
+    def device_step(pruned=False):
         tree = ctypes.c_void_p()
         core._check(core.lib.tsr_tree_build_device(ctypes.byref(dview), ctypes.byref(params), sptr,
                                                    ctypes.byref(tree)))
         occ = ctypes.c_void_p()
-        core._check(core.lib.tsr_occupancy_compute(tree, ctypes.byref(cams.view()), ctypes.byref(params), 0, sptr,
-                                                   ctypes.byref(occ)))
+        if pruned:
+            core._check(core.lib.tsr_occupancy_compute_pruned(tree, ctypes.byref(cams.view()), ctypes.byref(params),
+                                                              ctypes.byref(pruner_view), sptr, ctypes.byref(occ)))
+        else:
+            core._check(core.lib.tsr_occupancy_compute(tree, ctypes.byref(cams.view()), ctypes.byref(params), 0,
+                                                       sptr, ctypes.byref(occ)))
         mesh = ctypes.c_void_p()
         core._check(core.lib.tsr_dmc_extract(tree, occ, sptr, ctypes.byref(mesh)))
         tc = core.tsr_tree_counts()
@@ -359,6 +365,41 @@ def our_arm(args):
                                        "scaled to this run's units"},
         "clocks": clk,
     }
+    # ---- the learned pruner's field (same workload, same timing), judged by
+    # the plain method on this scene
+    if not args.no_pruned:
+        pr = core.Pruner.load()
+        pruner_view = pr.view()
+        for _ in range(max(1, args.warmup // 2)):
+            device_step(pruned=True)
+        barrier()
+        pev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(args.steps)]
+        pstage = np.zeros(16)
+        for i in range(args.steps):
+            pev[i][0].record(stream)
+            _, _, ptms, poms, poc = device_step(pruned=True)
+            pev[i][1].record(stream)
+            pstage += np.concatenate([ptms, poms])
+        barrier()
+        p_step_ms = [a.elapsed_time(b) for a, b in pev]
+        t_pruned = max_over_ranks(sum(p_step_ms) / 1e3)
+        from tsr_b200 import pruner as pruner_mod
+        jt = core.Tree(core.Samples(scene.pos, scene.nrm, scene.scale, scene.conf, scene.links), params,
+                       stream=stream, reorder_samples=False)
+        j = pruner_mod.judge(jt, cams, pr, params, stream=stream)
+        del jt
+        line["pruned"] = {
+            "value": world_samples * args.steps / t_pruned, "unit": UNIT, "ms_per_step": 1e3 * t_pruned / args.steps,
+            "step_ms": [round(x, 3) for x in p_step_ms],
+            "speedup_vs_plain": t_value / t_pruned,
+            "skipped_prior_queries": poc.pruned_leaves, "leaves": int(Nl),
+            "stage_ms": {k: round(float(v), 3) for k, v in zip(names, pstage / args.steps) if k},
+            "judge": {"sign_agreement": j["sign_agreement"], "case_agreement": j["case_agreement"],
+                      "vertex_hausdorff": j["vertex_hausdorff"], "finest_leaf_size": j["finest_leaf_size"],
+                      "triangles_plain_pruned": j["triangles"]},
+            "network": "tsr_b200/pruner_weights.npz (trained on 7 random CSG scenes of 1M samples, seeds 1-7)",
+        }
     if rank == 0 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         cs = cpu_scene(args.workload)
@@ -382,6 +423,7 @@ def main():
     ap.add_argument("--workload", default="csg4m", choices=["csg4m", "csg1m", "sphere", "heldout16m"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--value-only", action="store_true", help="skip the e2e leg (profiling runs)")
+    ap.add_argument("--no-pruned", action="store_true", help="skip the learned pruner's leg")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)

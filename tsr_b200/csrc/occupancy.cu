@@ -691,17 +691,26 @@ __global__ void __launch_bounds__(PT_BLOCK) k_priors_x(uint32_t nl, uint32_t nn,
         nvis += 8;
         if (d <= max_depth) {
 #pragma unroll
+            // every test for every child, without branches; only the outcome
+            // (a row to add, or a child to descend into) is conditional.  The
+            // rows of all eight children are loaded before any is added, so
+            // their L2 latencies overlap (adding 0 for the others is exact).
+            double2 v[8];
             for (int ci = 0; ci < 8; ++ci) {
-                // every test for every child, without branches; only the
-                // outcome (a row to add, or a child to descend into) is conditional
                 const bool flagged = (ry[ci] & REC_FLAG) != 0;
                 const bool leaf = rx[ci] == INVALID;
                 const D3 bmn = child_coords(x_min, cs, (uint32_t)ci);
                 const D3 bmx{dadd(bmn.x, cs), dadd(bmn.y, cs), dadd(bmn.z, cs)};
                 const bool meets = flagged && sphere_meets_box(bmn, bmx, center, radius);
                 const bool inside = can_add && box_inside_sphere(bmn, cs, center, radius);
-                if (meets && (inside || leaf)) add_row(x_c0 + ci, inside ? max_depth - d : 0u);
+                const size_t row = (size_t)(inside ? max_depth - d : 0u) * nn + x_c0 + ci;
+                v[ci] = (meets && (inside || leaf)) ? __ldg(&psum[row]) : make_double2(0.0, 0.0);
                 if (meets && !inside && !leaf && can_descend) mask |= 1u << ci;
+            }
+#pragma unroll
+            for (int ci = 0; ci < 8; ++ci) {
+                eL += v[ci].x;
+                sL += v[ci].y;
             }
         }
         if (mask) {
