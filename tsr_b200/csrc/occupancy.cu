@@ -437,18 +437,27 @@ __global__ void __launch_bounds__(PT_BLOCK, (TYPE == 0) ? 6 : 5) k_cone_x(uint64
         const F3 ctr0 = x_min + f3(h, h, h);
         uint32_t mask = 0;
         nvis += 8;
+        // the lanes expanding a node this step (the others wait at the loop top)
+        const unsigned act = __activemask();
 #pragma unroll
         for (int ci = 0; ci < 8; ++ci) {
             // both tests for every child, without branches; only the outcome
-            // (a leaf's kernel, or a child to descend into) is conditional
+            // (a leaf's kernel, or a child to descend into) is conditional.  A
+            // test is skipped only when no expanding lane needs it at this slot.
             const bool flagged = TYPE == SAMPLENESS || (ry[ci] & REC_FLAG);
             const bool leaf = rx[ci] == INVALID;
-            F3 ctr = f3((ci & 1) ? ctr0.x + size : ctr0.x, (ci & 2) ? ctr0.y + size : ctr0.y,
-                        (ci & 4) ? ctr0.z + size : ctr0.z);
-            float te, r2;
-            cone_coords(c, ctr, te, r2);
-            const float val = kernel_value(c, te, r2, TYPE == SAMPLENESS, fconf);
-            const bool sep = separated_at(c, te, r2, hs, dt);
+            const bool want_k = flagged && leaf, want_s = flagged && !leaf && can_descend;
+            const bool any_k = __any_sync(act, want_k), any_s = __any_sync(act, want_s);
+            float val = 0.0f;
+            bool sep = true;
+            if (any_k || any_s) {
+                F3 ctr = f3((ci & 1) ? ctr0.x + size : ctr0.x, (ci & 2) ? ctr0.y + size : ctr0.y,
+                            (ci & 4) ? ctr0.z + size : ctr0.z);
+                float te, r2;
+                cone_coords(c, ctr, te, r2);
+                if (any_k) val = kernel_value(c, te, r2, TYPE == SAMPLENESS, fconf);
+                if (any_s) sep = separated_at(c, te, r2, hs, dt);
+            }
             // a leaf: addKernel's exact test decides, no box test needed
             if (flagged && leaf && val > 0.0f) {
                 uint32_t lf = ry[ci] & REC_NOLEAF;
@@ -608,6 +617,7 @@ __global__ void __launch_bounds__(PT_BLOCK) k_priors_x(uint32_t nl, uint32_t nn,
     uint32_t l = 0, max_depth = 0;
     D3 center{0.0, 0.0, 0.0};
     double radius = 0.0, eL = 0.0, sL = 0.0;
+    float r2f = 0.0f;
     unsigned long long nvis = 0;
     auto add_row = [&](uint32_t n, uint32_t k) {
         double2 v = psum[(size_t)k * nn + n];
@@ -650,6 +660,7 @@ __global__ void __launch_bounds__(PT_BLOCK) k_priors_x(uint32_t nl, uint32_t nn,
                     double half = dmul(0.5, size);
                     center = D3{dadd(mn.x, half), dadd(mn.y, half), dadd(mn.z, half)};
                     radius = dmul(size, rel_radius);
+                    r2f = (float)dmul(radius, radius);
                     max_depth = ld + MAX_DEPTH_DIFFERENCE;
                     eL = sL = 0.0;
                     active = true;
@@ -690,19 +701,48 @@ __global__ void __launch_bounds__(PT_BLOCK) k_priors_x(uint32_t nl, uint32_t nn,
         uint32_t mask = 0;
         nvis += 8;
         if (d <= max_depth) {
-#pragma unroll
-            // every test for every child, without branches; only the outcome
+            // Every test for every child without branches; only the outcome
             // (a row to add, or a child to descend into) is conditional.  The
-            // rows of all eight children are loaded before any is added, so
-            // their L2 latencies overlap (adding 0 for the others is exact).
+            // exact FP64 tests run only where an FP32 estimate in the query
+            // centre's frame cannot decide: its error is bounded by e_a per
+            // axis (rounding of the frame offset and of two FP32 adds) plus
+            // 4e-7 of the squared distances, and a decision needs a margin
+            // of 1e-6 r^2 beyond that.  The rows of all eight children are
+            // loaded before any is added, so their L2 latencies overlap
+            // (adding 0 for the others is exact).
+            const float csf = (float)cs;
+            const float rx0 = (float)dsub(x_min.x, center.x), ry0 = (float)dsub(x_min.y, center.y),
+                        rz0 = (float)dsub(x_min.z, center.z);
+            const float ex = 4e-7f * (fabsf(rx0) + 2.0f * csf), ey = 4e-7f * (fabsf(ry0) + 2.0f * csf),
+                        ez = 4e-7f * (fabsf(rz0) + 2.0f * csf);
             double2 v[8];
+#pragma unroll
             for (int ci = 0; ci < 8; ++ci) {
                 const bool flagged = (ry[ci] & REC_FLAG) != 0;
                 const bool leaf = rx[ci] == INVALID;
-                const D3 bmn = child_coords(x_min, cs, (uint32_t)ci);
-                const D3 bmx{dadd(bmn.x, cs), dadd(bmn.y, cs), dadd(bmn.z, cs)};
-                const bool meets = flagged && sphere_meets_box(bmn, bmx, center, radius);
-                const bool inside = can_add && box_inside_sphere(bmn, cs, center, radius);
+                const float lx = (ci & 1) ? rx0 + csf : rx0, ly = (ci & 2) ? ry0 + csf : ry0,
+                            lz = (ci & 4) ? rz0 + csf : rz0;
+                const float hx = lx + csf, hy = ly + csf, hz = lz + csf;
+                const float tx = lx > 0.0f ? lx : (hx < 0.0f ? -hx : 0.0f);
+                const float ty = ly > 0.0f ? ly : (hy < 0.0f ? -hy : 0.0f);
+                const float tz = lz > 0.0f ? lz : (hz < 0.0f ? -hz : 0.0f);
+                const float d2 = tx * tx + ty * ty + tz * tz;
+                const float b1 = 2.0f * ((tx + ex) * ex + (ty + ey) * ey + (tz + ez) * ez) + 4e-7f * d2;
+                const float fx = fmaxf(fabsf(lx), fabsf(hx)), fy = fmaxf(fabsf(ly), fabsf(hy)),
+                            fz = fmaxf(fabsf(lz), fabsf(hz));
+                const float D2 = fx * fx + fy * fy + fz * fz;
+                const float b2 = 2.0f * ((fx + ex) * ex + (fy + ey) * ey + (fz + ez) * ez) + 4e-7f * D2;
+                bool meets = d2 + b1 < r2f * (1.0f - 1e-6f);
+                bool inside = can_add && (D2 + b2 < r2f * (1.0f - 2e-6f));
+                const bool meets_unsure = !meets && !(d2 - b1 > r2f * (1.0f + 1e-6f));
+                const bool inside_unsure = can_add && !inside && !(D2 - b2 > r2f * (1.0f + 1e-6f));
+                if (flagged && (meets_unsure || ((meets || meets_unsure) && inside_unsure))) {
+                    const D3 bmn = child_coords(x_min, cs, (uint32_t)ci);
+                    const D3 bmx{dadd(bmn.x, cs), dadd(bmn.y, cs), dadd(bmn.z, cs)};
+                    meets = sphere_meets_box(bmn, bmx, center, radius);
+                    inside = can_add && box_inside_sphere(bmn, cs, center, radius);
+                }
+                meets = meets && flagged;
                 const size_t row = (size_t)(inside ? max_depth - d : 0u) * nn + x_c0 + ci;
                 v[ci] = (meets && (inside || leaf)) ? __ldg(&psum[row]) : make_double2(0.0, 0.0);
                 if (meets && !inside && !leaf && can_descend) mask |= 1u << ci;
