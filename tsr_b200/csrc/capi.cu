@@ -44,6 +44,33 @@ static void keep_pool_memory() {
     done_mask.fetch_or(bit);
 }
 
+// Grows the device's default pool in one step to hold a call's working set.
+// Without it the pool grew piecemeal during the call whenever a large request
+// found no free block of its size, and each growth (mapping fresh memory)
+// stalled the host for 5-200 ms in the middle of a reconstruction.  The pool
+// keeps the memory (see keep_pool_memory), so later calls find it free.
+void reserve_pool(size_t want, cudaStream_t st) {
+    int dev = 0;
+    cudaMemPool_t pool;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return;
+    }
+    uint64_t reserved = 0, used = 0;
+    if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) != cudaSuccess ||
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return;
+    }
+    if (reserved >= used && reserved - used >= want) return;
+    void *p = nullptr;
+    if (cudaMallocAsync(&p, want, st) == cudaSuccess) {
+        (void)cudaFreeAsync(p, st);
+    } else {
+        (void)cudaGetLastError();   // not enough memory for the reservation: allocate as we go
+    }
+}
+
 template <class F>
 static tsr_status guarded(F &&f) {
     try {

@@ -72,6 +72,7 @@ void mlp_infer_bf16(const float *x, uint32_t n, const float *params, float *out,
 void pruner_predict(const tsr_tree &t, const tsr_pruner &pr, const double *esum, const double *ssum,
                     double threshold, DBuf<uint8_t> &pred, cudaStream_t st);
 void extract_dmc(const tsr_tree &t, const tsr_occupancy &o, tsr_mesh &m);
+void reserve_pool(size_t want, cudaStream_t st);
 void root_scope_noalloc(uint64_t count, const double *positions, const double *scales, double h_svo,
                         double *out_min_xyz_size, cudaStream_t st);
 }  // namespace tsr

@@ -437,27 +437,18 @@ __global__ void __launch_bounds__(PT_BLOCK, (TYPE == 0) ? 6 : 5) k_cone_x(uint64
         const F3 ctr0 = x_min + f3(h, h, h);
         uint32_t mask = 0;
         nvis += 8;
-        // the lanes expanding a node this step (the others wait at the loop top)
-        const unsigned act = __activemask();
 #pragma unroll
         for (int ci = 0; ci < 8; ++ci) {
             // both tests for every child, without branches; only the outcome
-            // (a leaf's kernel, or a child to descend into) is conditional.  A
-            // test is skipped only when no expanding lane needs it at this slot.
+            // (a leaf's kernel, or a child to descend into) is conditional
             const bool flagged = TYPE == SAMPLENESS || (ry[ci] & REC_FLAG);
             const bool leaf = rx[ci] == INVALID;
-            const bool want_k = flagged && leaf, want_s = flagged && !leaf && can_descend;
-            const bool any_k = __any_sync(act, want_k), any_s = __any_sync(act, want_s);
-            float val = 0.0f;
-            bool sep = true;
-            if (any_k || any_s) {
-                F3 ctr = f3((ci & 1) ? ctr0.x + size : ctr0.x, (ci & 2) ? ctr0.y + size : ctr0.y,
-                            (ci & 4) ? ctr0.z + size : ctr0.z);
-                float te, r2;
-                cone_coords(c, ctr, te, r2);
-                if (any_k) val = kernel_value(c, te, r2, TYPE == SAMPLENESS, fconf);
-                if (any_s) sep = separated_at(c, te, r2, hs, dt);
-            }
+            F3 ctr = f3((ci & 1) ? ctr0.x + size : ctr0.x, (ci & 2) ? ctr0.y + size : ctr0.y,
+                        (ci & 4) ? ctr0.z + size : ctr0.z);
+            float te, r2;
+            cone_coords(c, ctr, te, r2);
+            const float val = kernel_value(c, te, r2, TYPE == SAMPLENESS, fconf);
+            const bool sep = separated_at(c, te, r2, hs, dt);
             // a leaf: addKernel's exact test decides, no box test needed
             if (flagged && leaf && val > 0.0f) {
                 uint32_t lf = ry[ci] & REC_NOLEAF;
@@ -839,6 +830,9 @@ void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_
     o.n_leaves = nl;
     o.n_nodes = nn;
     o.confidence_threshold = p.confidence_threshold;
+    // working set: per link the set-up record, keys and order; per node the
+    // traversal records, states and the prior table; per leaf the sums
+    reserve_pool((size_t)t.n_samples * t.k * 160 + (size_t)nn * 200 + (size_t)nl * 120 + (64u << 20), o.stream);
     Timer timer(st);
     DBuf<D3> cams(cv.count, st);
     if (cv.count) TSR_CUDA(cudaMemcpyAsync(cams.p, cv.positions, (size_t)cv.count * 24, cudaMemcpyHostToDevice, st));

@@ -989,6 +989,9 @@ void build_tree(tsr_tree &t, const tsr_samples_view &sv, bool on_device) {
     const double h_svo = t.params.max_relative_sampling_distance;
     t.n_samples = n;
     t.k = k;
+    // working set of the build: samples twice (input and tree order), the
+    // sampling rounds' per-side buffers, the node store and its relayout
+    reserve_pool((size_t)n * (700 + 8 * k) + (64u << 20), st);
     EventTimer timer(st);
 
     // ---- upload samples (FP64, Real = double)
