@@ -85,17 +85,19 @@ __device__ __forceinline__ float kernel_value(const ConeF &c, float te, float r2
     return ok ? scaled : 0.0f;
 }
 
-// Cone-frame coordinates of point x: te and the squared distance to the axis.
-__device__ __forceinline__ void cone_coords(const ConeF &c, F3 x, float &te, float &r2) {
+// Cone-frame coordinates of point x: te, the squared distance to the axis
+// and the L1 norm of the offset from the axis.
+__device__ __forceinline__ void cone_coords(const ConeF &c, F3 x, float &te, float &r2, float &q1) {
     F3 u = x - c.end;
     te = fdot(u, c.m) * c.inv_denom;
     F3 q = u - c.axis * te;
     r2 = fdot(q, q);
+    q1 = fabsf(q.x) + fabsf(q.y) + fabsf(q.z);
 }
 
 __device__ inline float eval_kernel(const ConeF &c, F3 x, bool sampleness, float conf) {
-    float te, r2;
-    cone_coords(c, x, te, r2);
+    float te, r2, q1;
+    cone_coords(c, x, te, r2, q1);
     return kernel_value(c, te, r2, sampleness, conf);
 }
 
@@ -127,16 +129,21 @@ __device__ inline bool cone_box_separated_pt(const ConeF &c, F3 bmin, float size
     return bound > tmax * c.radius * 1.0001f + 1e-4f * (qn + hs + dt * c.full);
 }
 
-// The same test for a box of centre coordinates (te, r2) and half size hs
-// already widened by the recurrence slack; dt = hs * |m|_1 * |1/denom|.
-// The last comparison, qn - 1e-4 qn > k with qn = sqrt(r2), is taken on
-// squares (k > 0 whenever it is reached).  Straight-line code.
-__device__ __forceinline__ bool separated_at(const ConeF &c, float te, float r2, float hs, float dt) {
+// The same test for a box of centre coordinates (te, r2, q1 = |q|_1 of the
+// offset q from the axis) and half size hs already widened by the recurrence
+// slack; dt = hs * |m|_1 * |1/denom|.  Every box point is at least
+// |q| - hs |q|_1 / |q| - dt * full from the axis (the box's extent along the
+// unit offset direction, plus the axis shift over its te range), which is
+// tighter than the circumscribed sphere's |q| - sqrt(3) hs.  Straight-line
+// code; |q| = 0 never separates.
+__device__ __forceinline__ bool separated_at(const ConeF &c, float te, float r2, float q1, float hs, float dt) {
     const float slack = 1e-4f * (dt + fabsf(te)) + 1e-6f;
     bool sep = (te + dt < c.t_start_e - slack) | (te - dt >= slack) | (1.0f + te + dt <= 0.0f);
     const float tmax = fminf(1.0f + te + dt, 1.0f);
-    const float k = hs * 1.7320508f + dt * c.full + tmax * c.radius * 1.0001f + 1e-4f * (hs + dt * c.full);
-    sep |= (k > 0.0f) & (r2 * 0.99980001f > k * k);
+    const float inv = rsqrtf(r2);
+    const float qn = r2 * inv;
+    const float rest = dt * c.full + tmax * c.radius * 1.0001f + 1e-4f * (hs + dt * c.full);
+    sep |= (qn * 0.9999f - hs * q1 * inv) > rest;
     return sep;
 }
 
@@ -445,10 +452,10 @@ __global__ void __launch_bounds__(PT_BLOCK, (TYPE == 0) ? 6 : 5) k_cone_x(uint64
             const bool leaf = rx[ci] == INVALID;
             F3 ctr = f3((ci & 1) ? ctr0.x + size : ctr0.x, (ci & 2) ? ctr0.y + size : ctr0.y,
                         (ci & 4) ? ctr0.z + size : ctr0.z);
-            float te, r2;
-            cone_coords(c, ctr, te, r2);
+            float te, r2, q1;
+            cone_coords(c, ctr, te, r2, q1);
             const float val = kernel_value(c, te, r2, TYPE == SAMPLENESS, fconf);
-            const bool sep = separated_at(c, te, r2, hs, dt);
+            const bool sep = separated_at(c, te, r2, q1, hs, dt);
             // a leaf: addKernel's exact test decides, no box test needed
             if (flagged && leaf && val > 0.0f) {
                 uint32_t lf = ry[ci] & REC_NOLEAF;
