@@ -85,19 +85,19 @@ __device__ __forceinline__ float kernel_value(const ConeF &c, float te, float r2
     return ok ? scaled : 0.0f;
 }
 
-// Cone-frame coordinates of point x: te, the squared distance to the axis
-// and the L1 norm of the offset from the axis.
-__device__ __forceinline__ void cone_coords(const ConeF &c, F3 x, float &te, float &r2, float &q1) {
+// Cone-frame coordinates of point x: te, the offset q from the axis point of
+// the same te, and |q|^2.
+__device__ __forceinline__ void cone_coords(const ConeF &c, F3 x, float &te, F3 &q, float &r2) {
     F3 u = x - c.end;
     te = fdot(u, c.m) * c.inv_denom;
-    F3 q = u - c.axis * te;
+    q = u - c.axis * te;
     r2 = fdot(q, q);
-    q1 = fabsf(q.x) + fabsf(q.y) + fabsf(q.z);
 }
 
 __device__ inline float eval_kernel(const ConeF &c, F3 x, bool sampleness, float conf) {
-    float te, r2, q1;
-    cone_coords(c, x, te, r2, q1);
+    float te, r2;
+    F3 q;
+    cone_coords(c, x, te, q, r2);
     return kernel_value(c, te, r2, sampleness, conf);
 }
 
@@ -129,21 +129,24 @@ __device__ inline bool cone_box_separated_pt(const ConeF &c, F3 bmin, float size
     return bound > tmax * c.radius * 1.0001f + 1e-4f * (qn + hs + dt * c.full);
 }
 
-// The same test for a box of centre coordinates (te, r2, q1 = |q|_1 of the
-// offset q from the axis) and half size hs already widened by the recurrence
-// slack; dt = hs * |m|_1 * |1/denom|.  Every box point is at least
-// |q| - hs |q|_1 / |q| - dt * full from the axis (the box's extent along the
-// unit offset direction, plus the axis shift over its te range), which is
-// tighter than the circumscribed sphere's |q| - sqrt(3) hs.  Straight-line
-// code; |q| = 0 never separates.
-__device__ __forceinline__ bool separated_at(const ConeF &c, float te, float r2, float q1, float hs, float dt) {
+// The same test for a box of centre coordinates (te, q, r2 = |q|^2; q is
+// the offset from the axis point of the same te) and half size hs already
+// widened by the recurrence slack; dt = hs * |m|_1 * |1/denom|.  A box point
+// ctr + d has te + (d.m)/denom and offset q + d - axis (d.m)/denom, whose
+// length is at least |q| + d.w with w = (q - (q.axis / denom) m) / |q|, so
+// every box point is at least |q| - hs |w|_1 from the axis: the exact
+// support of the box in that direction, with the axis shift over the box's
+// te range folded in.  Straight-line code; |q| = 0 never separates.
+__device__ __forceinline__ bool separated_at(const ConeF &c, float te, F3 q, float r2, float hs, float dt) {
     const float slack = 1e-4f * (dt + fabsf(te)) + 1e-6f;
     bool sep = (te + dt < c.t_start_e - slack) | (te - dt >= slack) | (1.0f + te + dt <= 0.0f);
     const float tmax = fminf(1.0f + te + dt, 1.0f);
     const float inv = rsqrtf(r2);
     const float qn = r2 * inv;
-    const float rest = dt * c.full + tmax * c.radius * 1.0001f + 1e-4f * (hs + dt * c.full);
-    sep |= (qn * 0.9999f - hs * q1 * inv) > rest;
+    const F3 v = q - c.m * (fdot(q, c.axis) * c.inv_denom);
+    const float v1 = fabsf(v.x) + fabsf(v.y) + fabsf(v.z);
+    const float rest = tmax * c.radius * 1.0001f + 1e-4f * (hs + dt * c.full);
+    sep |= (qn * 0.9999f - hs * v1 * inv) > rest;
     return sep;
 }
 
@@ -452,10 +455,11 @@ __global__ void __launch_bounds__(PT_BLOCK, (TYPE == 0) ? 6 : 5) k_cone_x(uint64
             const bool leaf = rx[ci] == INVALID;
             F3 ctr = f3((ci & 1) ? ctr0.x + size : ctr0.x, (ci & 2) ? ctr0.y + size : ctr0.y,
                         (ci & 4) ? ctr0.z + size : ctr0.z);
-            float te, r2, q1;
-            cone_coords(c, ctr, te, r2, q1);
+            float te, r2;
+            F3 q;
+            cone_coords(c, ctr, te, q, r2);
             const float val = kernel_value(c, te, r2, TYPE == SAMPLENESS, fconf);
-            const bool sep = separated_at(c, te, r2, q1, hs, dt);
+            const bool sep = separated_at(c, te, q, r2, hs, dt);
             // a leaf: addKernel's exact test decides, no box test needed
             if (flagged && leaf && val > 0.0f) {
                 uint32_t lf = ry[ci] & REC_NOLEAF;
