@@ -155,6 +155,13 @@ TSR_API tsr_status tsr_tree_build(const tsr_samples_view *samples, const tsr_par
 TSR_API tsr_status tsr_tree_build_device(const tsr_samples_view *samples, const tsr_params *params,
                                          void *cuda_stream, tsr_tree **out_tree);
 TSR_API void tsr_tree_free(tsr_tree *tree);
+/* Tree::eraseSamples (Tree.cpp:50-53, Nodes.cpp:644-671) plus Samples::compact
+ * (Samples.cpp) of the tree's own samples: `inliers` (HOST, one byte per
+ * sample in tree order, nonzero = keep).  Node sample counts and start indices
+ * follow the compaction; the topology is unchanged; the permutation maps
+ * erased input samples to 0xFFFFFFFF.  Scene::eraseSamples (Scene.cpp:270-307)
+ * calls tsr_occupancy_update(..., for_removal = 1, outliers) first. */
+TSR_API tsr_status tsr_tree_erase_samples(tsr_tree *tree, const uint8_t *inliers);
 TSR_API tsr_status tsr_tree_get_counts(const tsr_tree *tree, tsr_tree_counts *out);
 TSR_API tsr_status tsr_tree_root_scope(const tsr_tree *tree, double min_xyz_size[4]);
 /* The root scope tsr_tree_build would give these samples (min corner xyz and
@@ -194,6 +201,17 @@ TSR_API tsr_status tsr_occupancy_compute(const tsr_tree *tree, const tsr_cameras
                                  const tsr_params *params, int mode, void *cuda_stream,
                                  tsr_occupancy **out_occupancy);
 TSR_API void tsr_occupancy_free(tsr_occupancy *occ);
+/* Occupancy::addSamples / eraseSamples (Occupancy.h:167-175) ->
+ * onSamplesChanged (Occupancy.cpp:129-136): the kernels of the links of
+ * `samples` (HOST indices in tree order, i.e. the order tsr_tree_copy_samples
+ * returns) are added (for_removal = 0) or removed (for_removal = 1) from the
+ * field's sums, lengths and cone count (removal keeps node flags, like the
+ * reference), then every prior and occupancy value is recomputed
+ * (Occupancy::update, Occupancy.h:222-227).  The tree must be the one the
+ * field was computed on; the work counters then describe this update. */
+TSR_API tsr_status tsr_occupancy_update(tsr_occupancy *occ, const tsr_tree *tree, const tsr_cameras_view *cameras,
+                                        const tsr_params *params, int for_removal, const uint32_t *samples,
+                                        uint32_t count, void *cuda_stream);
 /* Work counters of the last field computation (no counterpart in the
  * reference; instrumentation). */
 TSR_API tsr_status tsr_occupancy_get_counts(const tsr_occupancy *occ, tsr_occupancy_counts *out);

@@ -100,6 +100,8 @@ _sig = {
     "tsr_mesh_get_counts": (ctypes.c_int, [_P, _P]),
     "tsr_mesh_copy": (ctypes.c_int, [_P, _P, _P, _P, _P, _P]),
     "tsr_occupancy_leaf_features": (ctypes.c_int, [_P, _P, _P]),
+    "tsr_occupancy_update": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_int, _P, ctypes.c_uint32, _P]),
+    "tsr_tree_erase_samples": (ctypes.c_int, [_P, _P]),
     "tsr_mlp_train_batch": (ctypes.c_int, [_P, _P, ctypes.c_uint32, _P, _P, _P, ctypes.c_float, ctypes.c_float,
                                            _P]),
     "tsr_mlp_adam": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_uint32, ctypes.c_float, ctypes.c_float, _P]),
@@ -272,6 +274,7 @@ class Tree:
         _check(lib.tsr_tree_get_counts(self._h, ctypes.byref(c)))
         self.counts = {k: int(getattr(c, k)) for k, _ in tsr_tree_counts._fields_}
         self.sample_count = samples.count
+        self.input_count = samples.count
         if reorder_samples:
             # the reference reorders Samples in place (Nodes.cpp:630); copy the
             # device-side reordered arrays back instead of permuting on the host
@@ -301,8 +304,19 @@ class Tree:
         m = self.getRootScope()
         return m[:3] + 0.5 * m[3]
 
+    def eraseSamples(self, inliers):
+        """Tree::eraseSamples (Tree.cpp:50-53) with the samples' compaction;
+        ``inliers``: one bool per sample in tree order."""
+        keep = np.ascontiguousarray(inliers, np.uint8)
+        if keep.shape[0] != self.sample_count:
+            raise ValueError("one flag per sample expected")
+        _check(lib.tsr_tree_erase_samples(self._h, _ptr(keep)))
+        self.sample_count = int(keep.astype(bool).sum())
+        self._nodes = None
+
     def getPermutation(self):
-        t = np.zeros(self.sample_count, np.uint32)
+        """Tree-order index of every input sample (0xFFFFFFFF once erased)."""
+        t = np.zeros(self.input_count, np.uint32)
         _check(lib.tsr_tree_copy_permutation(self._h, _ptr(t)))
         return t
 
@@ -380,6 +394,24 @@ class Occupancy:
     @property
     def handle(self):
         return self._h
+
+    def addSamples(self, samples, cameras, params=None):
+        """Occupancy::addSamples (Occupancy.h:167-170): tree-order indices."""
+        self._on_samples_changed(False, samples, cameras, params)
+
+    def eraseSamples(self, samples, cameras, params=None):
+        """Occupancy::eraseSamples (Occupancy.h:172-175): tree-order indices."""
+        self._on_samples_changed(True, samples, cameras, params)
+
+    def _on_samples_changed(self, removal, samples, cameras, params):
+        ids = np.ascontiguousarray(samples, np.uint32)
+        p = params or self.tree.params
+        _check(lib.tsr_occupancy_update(self._h, self.tree.handle, ctypes.byref(cameras.view()), ctypes.byref(p),
+                                        1 if removal else 0, _ptr(ids), ids.shape[0], _stream_ptr(self._stream)))
+        self._cache = {}
+        c = tsr_occupancy_counts()
+        _check(lib.tsr_occupancy_get_counts(self._h, ctypes.byref(c)))
+        self.counts = {k: int(getattr(c, k)) for k, _ in tsr_occupancy_counts._fields_}
 
     def getLeafFeatures(self):
         """The learned pruner's per-leaf features (leaves x 10 float32)."""

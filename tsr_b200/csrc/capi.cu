@@ -226,7 +226,7 @@ tsr_status tsr_tree_copy_samples(const tsr_tree *t, double *positions, double *n
 tsr_status tsr_tree_copy_permutation(const tsr_tree *t, uint32_t *target) {
     return guarded([&] {
         if (!t || !target) fail(TSR_ERR_INVALID_ARG, "null argument");
-        to_host(t->target, t->n_samples, target, t->stream);
+        to_host(t->target, t->target.n, target, t->stream);   // one entry per input sample
         TSR_CUDA(cudaStreamSynchronize(t->stream));
     });
 }
@@ -376,6 +376,36 @@ tsr_status tsr_mlp_infer_bf16(const float *x, uint32_t n, const float *params, f
     return guarded([&] {
         if (!x || !params || !logits) fail(TSR_ERR_INVALID_ARG, "null argument");
         mlp_infer_bf16(x, n, params, logits, (cudaStream_t)cuda_stream);
+    });
+}
+
+tsr_status tsr_occupancy_update(tsr_occupancy *o, const tsr_tree *tree, const tsr_cameras_view *cameras,
+                                const tsr_params *params, int for_removal, const uint32_t *samples, uint32_t count,
+                                void *cuda_stream) {
+    return guarded([&] {
+        if (!o || !tree || !cameras || (count && !samples)) fail(TSR_ERR_INVALID_ARG, "null argument");
+        if (o->n_leaves != tree->n_leaves || o->n_nodes != tree->n_nodes)
+            fail(TSR_ERR_INVALID_ARG, "field of another tree");
+        if (cameras->count && !cameras->positions) fail(TSR_ERR_INVALID_ARG, "null camera positions");
+        for (uint32_t i = 0; i < count; ++i)
+            if (samples[i] >= tree->n_samples) fail(TSR_ERR_INVALID_ARG, "sample index out of range");
+        tsr_params p = tree->params;
+        if (params) p = *params;
+        check_params(p);
+        o->stream = (cudaStream_t)cuda_stream;
+        DBuf<uint32_t> chosen(count, o->stream);
+        if (count)
+            TSR_CUDA(cudaMemcpyAsync(chosen.p, samples, (size_t)count * 4, cudaMemcpyHostToDevice, o->stream));
+        compute_occupancy(*tree, *cameras, p, 0, *o, nullptr, chosen.p, count, for_removal ? -1.0 : 1.0, true);
+    });
+}
+
+tsr_status tsr_tree_erase_samples(tsr_tree *t, const uint8_t *inliers) {
+    return guarded([&] {
+        if (!t || !inliers) fail(TSR_ERR_INVALID_ARG, "null argument");
+        DBuf<uint8_t> in(t->n_samples, t->stream);
+        TSR_CUDA(cudaMemcpyAsync(in.p, inliers, t->n_samples, cudaMemcpyHostToDevice, t->stream));
+        erase_tree_samples(*t, in.p);
     });
 }
 

@@ -60,7 +60,9 @@ struct tsr_mesh {
 namespace tsr {
 void build_tree(tsr_tree &t, const tsr_samples_view &sv, bool on_device);
 void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_params &p, int mode,
-                       tsr_occupancy &o, const tsr_pruner *pruner = nullptr);
+                       tsr_occupancy &o, const tsr_pruner *pruner = nullptr, const uint32_t *chosen = nullptr,
+                       uint32_t nchosen = 0, double sign = 1.0, bool update = false);
+void erase_tree_samples(tsr_tree &t, const uint8_t *inliers_dev);
 void leaf_features(const tsr_tree &t, const double *esum, const double *ssum, double threshold, DBuf<float> &feat,
                    cudaStream_t st);
 void mlp_train_batch(const float *x, const float *y, uint32_t n, const float *params, float *grads, float *loss,

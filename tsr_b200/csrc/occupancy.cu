@@ -240,10 +240,13 @@ __device__ __forceinline__ ConeF cone_of(const LinkRec &r) {
 
 // Set-up of link order[i] (Occupancy.cpp:174-201), FP64, and the start of its
 // traversal: the deepest node containing the cut cone's bounding box.
+// sign: +1 adds the links' kernels, -1 removes them (Occupancy::updateKernels
+// with forRemoval, Occupancy.cpp:138-248: the same acceptance, negated
+// values, cone lengths and cone count).
 template <int TYPE>
 __global__ void __launch_bounds__(128) k_link_setup(uint64_t nlinks, const uint32_t *order, LinkIn in, TreeIn tr,
                                                     const uint2 *rec, LinkRec *out, double *ksum, double *clen,
-                                                    double *cone_count, unsigned long long *accepted) {
+                                                    double *cone_count, unsigned long long *accepted, double sign) {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     double count = 0.0;
     unsigned long long acc = 0;
@@ -277,7 +280,7 @@ __global__ void __launch_bounds__(128) k_link_setup(uint64_t nlinks, const uint3
             double denom = axis.x * m.x + axis.y * m.y + axis.z * m.z;
             if (!(full > EPS) || !(kernel_r > 0.0) || fabs(denom) <= EPS * full) break;   // isDegenerated
             double conf = in.conf[s];
-            if (TYPE == EMPTINESS) count += conf;
+            if (TYPE == EMPTINESS) count += sign * conf;
             const double wlen = conf * length;
             const float fconf = (float)conf;
             const uint32_t max_depth =
@@ -327,8 +330,8 @@ __global__ void __launch_bounds__(128) k_link_setup(uint64_t nlinks, const uint3
                 float val = eval_kernel(c, smin + f3(h, h, h), TYPE == SAMPLENESS, fconf);
                 if (val > 0.0f) {
                     uint32_t leaf = srec.y & REC_NOLEAF;
-                    atomicAdd(&ksum[leaf], (double)val);
-                    atomicAdd(&clen[leaf], wlen);
+                    atomicAdd(&ksum[leaf], sign * (double)val);
+                    atomicAdd(&clen[leaf], sign * wlen);
                     ++acc;
                 }
                 break;
@@ -341,7 +344,7 @@ __global__ void __launch_bounds__(128) k_link_setup(uint64_t nlinks, const uint3
             r.a_over_l = c.a_over_l; r.t_start_e = c.t_start_e; r.n1 = c.n1;
             r.smin[0] = smin.x; r.smin[1] = smin.y; r.smin[2] = smin.z;
             r.fconf = fconf;
-            r.wlen = wlen;
+            r.wlen = sign * wlen;
             r.c0 = srec.x;
             r.depths = (base + 1) | (max_depth << 8);
             r.spos[0] = p.x; r.spos[1] = p.y; r.spos[2] = p.z;
@@ -367,7 +370,8 @@ __global__ void __launch_bounds__(PT_BLOCK, (TYPE == 0) ? 6 : 5) k_cone_x(uint64
                                                                          float root_size_f, double *ksum,
                                                                          double *clen, unsigned long long *accepted,
                                                                          unsigned long long *next_link,
-                                                                         unsigned long long *visits, int *err) {
+                                                                         unsigned long long *visits, int *err,
+                                                                         double sign) {
     const unsigned FULL = 0xffffffffu;
     const unsigned lane = threadIdx.x & 31;
     // stack of expanded nodes that still have children to descend into
@@ -463,8 +467,8 @@ __global__ void __launch_bounds__(PT_BLOCK, (TYPE == 0) ? 6 : 5) k_cone_x(uint64
             // a leaf: addKernel's exact test decides, no box test needed
             if (flagged && leaf && val > 0.0f) {
                 uint32_t lf = ry[ci] & REC_NOLEAF;
-                atomicAdd(&ksum[lf], (double)val);
-                atomicAdd(&clen[lf], wlen);
+                atomicAdd(&ksum[lf], sign * (double)val);
+                atomicAdd(&clen[lf], wlen);   // wlen carries the sign
                 ++acc;
             }
             if (flagged && !leaf && can_descend && !sep) mask |= 1u << ci;
@@ -512,13 +516,22 @@ __global__ void k_leaf_flags(uint32_t nl, const uint32_t *leaf_node, const doubl
     if (ksum[l] > 0.0) states[leaf_node[l]] |= flag;
 }
 
-__global__ void k_link_cameras(uint64_t nlinks, const uint32_t *links, uint32_t ncams, uint32_t *keys,
-                               uint32_t *vals) {
-    uint64_t l = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (l >= nlinks) return;
+// Camera of every listed link (list == null: links 0 .. nlinks-1), as sort keys.
+__global__ void k_link_cameras(uint64_t nlinks, const uint32_t *list, const uint32_t *links, uint32_t ncams,
+                               uint32_t *keys, uint32_t *vals) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nlinks) return;
+    const uint32_t l = list ? list[i] : (uint32_t)i;
     uint32_t c = links[l];
-    keys[l] = (c == INVALID || c >= ncams) ? ncams : c;
-    vals[l] = (uint32_t)l;
+    keys[i] = (c == INVALID || c >= ncams) ? ncams : c;
+    vals[i] = l;
+}
+
+// The links of the chosen samples: sample s has links s K .. s K + K - 1.
+__global__ void k_sample_links(uint32_t count, const uint32_t *samples, uint32_t k, uint32_t *out) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (uint64_t)count * k) return;
+    out[i] = samples[i / k] * k + (uint32_t)(i % k);
 }
 
 // forwardAnyChildStateFlag, one level bottom-up.
@@ -833,25 +846,42 @@ struct Timer {
 
 }  // namespace
 
+// The field of all links (update == false), or an update of an existing
+// field by the links of `chosen` samples (device indices, tree order) added
+// (sign +1) or removed (sign -1): Occupancy::update (Occupancy.h:222-227)
+// after onSamplesChanged (Occupancy.cpp:129-136) -- both cone passes over the
+// chosen links into the field's sums, node flags set only when adding, then
+// the priors and the occupancy of every leaf again.
 void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_params &p, int mode,
-                       tsr_occupancy &o, const tsr_pruner *pruner) {
+                       tsr_occupancy &o, const tsr_pruner *pruner, const uint32_t *chosen, uint32_t nchosen,
+                       double sign, bool update) {
     (void)mode;
     cudaStream_t st = o.stream;
     const uint32_t nl = t.n_leaves, nn = t.n_nodes;
     o.n_leaves = nl;
     o.n_nodes = nn;
     o.confidence_threshold = p.confidence_threshold;
+    const uint64_t nlinks = update ? (uint64_t)nchosen * t.k : (uint64_t)t.n_samples * t.k;
     // working set: per link the set-up record, keys and order; per node the
     // traversal records, states and the prior table; per leaf the sums
-    reserve_pool((size_t)t.n_samples * t.k * 160 + (size_t)nn * 200 + (size_t)nl * 120 + (64u << 20), o.stream);
+    reserve_pool((size_t)nlinks * 160 + (size_t)nn * 200 + (size_t)nl * 120 + (64u << 20), o.stream);
     Timer timer(st);
     DBuf<D3> cams(cv.count, st);
     if (cv.count) TSR_CUDA(cudaMemcpyAsync(cams.p, cv.positions, (size_t)cv.count * 24, cudaMemcpyHostToDevice, st));
-    DBuf<double> acc(4ull * nl, st);   // esum, ssum, elen, slen
-    acc.zero();
-    double *esum = acc.p, *ssum = acc.p + nl, *elen = acc.p + 2ull * nl, *slen = acc.p + 3ull * nl;
-    o.states.alloc(nn, st);
-    o.states.zero();
+    DBuf<double> acc;   // esum, ssum, elen, slen of a new field
+    double *esum, *ssum, *elen, *slen;
+    DBuf<uint32_t> link_list;
+    if (update) {
+        esum = o.e_sum.p; ssum = o.s_sum.p; elen = o.e_len.p; slen = o.s_len.p;
+        link_list.alloc(nlinks, st);
+        k_sample_links<<<grid_for(nlinks, BLK), BLK, 0, st>>>(nchosen, chosen, t.k, link_list.p); ::tsr::note_launch();
+    } else {
+        acc.alloc(4ull * nl, st);
+        acc.zero();
+        esum = acc.p; ssum = acc.p + nl; elen = acc.p + 2ull * nl; slen = acc.p + 3ull * nl;
+        o.states.alloc(nn, st);
+        o.states.zero();
+    }
     DBuf<double> cone_count(1, st);
     cone_count.zero();
     DBuf<unsigned long long> accepted(5, st);   // accepted E, S; visits E, S; prior visits
@@ -862,8 +892,7 @@ void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_
     LinkIn in{t.pos.p, t.nrm.p, t.scale.p, t.conf.p, t.links.p, cams.p, t.k, cv.count,
               p.max_relative_sampling_distance, p.bandwidth_factor, p.relative_sample_cone_length, t.root_size};
     TreeIn tr{t.nmin.p};
-    uint64_t nlinks = (uint64_t)t.n_samples * t.k;
-    o.links = nlinks;
+    if (!update) o.links = nlinks;
     DBuf<unsigned long long> next_link(1, st);
     unsigned x_grid = 0, prior_grid = 0;
     {
@@ -881,26 +910,40 @@ void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_
     next_link.zero();
     k_pack_rec<<<grid_for(nn, BLK), BLK, 0, st>>>(nn, t.children.p, t.node_to_leaf.p, nullptr, recs.p); ::tsr::note_launch();
     DBuf<LinkRec> lrec((size_t)nlinks, st);
-    k_link_setup<SAMPLENESS><<<grid_for(nlinks, 128), 128, 0, st>>>(nlinks, nullptr, in, tr, recs.p, lrec.p, ssum,
-                                                                    slen, cone_count.p, accepted.p + 1);
-    ::tsr::note_launch();
-    k_cone_x<SAMPLENESS><<<x_grid, PT_BLOCK, 0, st>>>(nlinks, lrec.p, tr, recs.p, (float)t.root_size, ssum, slen,
-                                                     accepted.p + 1, next_link.p, accepted.p + 3, err.p);
-    ::tsr::note_launch();
-    k_leaf_flags<<<grid_for(nl, BLK), BLK, 0, st>>>(nl, t.leaf_node.p, ssum, o.states.p, FLAG_SAMPLENESS); ::tsr::note_launch();
+    if (nlinks) {
+        k_link_setup<SAMPLENESS><<<grid_for(nlinks, 128), 128, 0, st>>>(nlinks, link_list.p, in, tr, recs.p, lrec.p,
+                                                                        ssum, slen, cone_count.p, accepted.p + 1,
+                                                                        sign);
+        ::tsr::note_launch();
+        k_cone_x<SAMPLENESS><<<x_grid, PT_BLOCK, 0, st>>>(nlinks, lrec.p, tr, recs.p, (float)t.root_size, ssum, slen,
+                                                         accepted.p + 1, next_link.p, accepted.p + 3, err.p, sign);
+        ::tsr::note_launch();
+    }
+    // flags mark leaves that received a kernel; removal leaves them set (Occupancy.cpp:232)
+    if (sign > 0.0) {
+        k_leaf_flags<<<grid_for(nl, BLK), BLK, 0, st>>>(nl, t.leaf_node.p, ssum, o.states.p, FLAG_SAMPLENESS);
+        ::tsr::note_launch();
+    }
     o.stage_ms[0] = timer.lap();
     // EMPTINESS links grouped by camera (stable, so sample order is kept
     // within a camera): a warp's cones then share their apex
     DBuf<uint32_t> order((size_t)nlinks, st);
     {
         DBuf<uint32_t> ckeys((size_t)nlinks, st), ckeys2((size_t)nlinks, st), vals((size_t)nlinks, st);
-        k_link_cameras<<<grid_for(nlinks, BLK), BLK, 0, st>>>(nlinks, t.links.p, cv.count, ckeys.p, vals.p); ::tsr::note_launch();
+        if (nlinks) {
+            k_link_cameras<<<grid_for(nlinks, BLK), BLK, 0, st>>>(nlinks, link_list.p, t.links.p, cv.count, ckeys.p,
+                                                                  vals.p); ::tsr::note_launch();
+        }
         int bits = 1;
         while ((1u << bits) <= cv.count) ++bits;
         size_t tmp = 0;
-        TSR_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, ckeys.p, ckeys2.p, vals.p, order.p, (int)nlinks, 0, bits, st));
-        DBuf<uint8_t> tb(tmp, st);
-        TSR_CUDA(cub::DeviceRadixSort::SortPairs(tb.p, tmp, ckeys.p, ckeys2.p, vals.p, order.p, (int)nlinks, 0, bits, st));
+        if (nlinks) {
+            TSR_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, ckeys.p, ckeys2.p, vals.p, order.p, (int)nlinks, 0,
+                                                     bits, st));
+            DBuf<uint8_t> tb(tmp, st);
+            TSR_CUDA(cub::DeviceRadixSort::SortPairs(tb.p, tmp, ckeys.p, ckeys2.p, vals.p, order.p, (int)nlinks, 0,
+                                                     bits, st));
+        }
     }
     // forwardAnyChildStateFlag(0, SAMPLENESS) before the EMPTINESS pass (Occupancy.cpp:141-142)
     for (int d = (int)t.level_start.size() - 2; d >= 0; --d) {
@@ -912,13 +955,18 @@ void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_
     ::tsr::note_launch();
     o.stage_ms[1] = timer.lap();
     next_link.zero();
-    k_link_setup<EMPTINESS><<<grid_for(nlinks, 128), 128, 0, st>>>(nlinks, order.p, in, tr, recs.p, lrec.p, esum,
-                                                                   elen, cone_count.p, accepted.p);
-    ::tsr::note_launch();
-    k_cone_x<EMPTINESS><<<x_grid, PT_BLOCK, 0, st>>>(nlinks, lrec.p, tr, recs.p, (float)t.root_size, esum, elen,
-                                                    accepted.p, next_link.p, accepted.p + 2, err.p);
-    ::tsr::note_launch();
-    k_leaf_flags<<<grid_for(nl, BLK), BLK, 0, st>>>(nl, t.leaf_node.p, esum, o.states.p, FLAG_EMPTINESS); ::tsr::note_launch();
+    if (nlinks) {
+        k_link_setup<EMPTINESS><<<grid_for(nlinks, 128), 128, 0, st>>>(nlinks, order.p, in, tr, recs.p, lrec.p, esum,
+                                                                       elen, cone_count.p, accepted.p, sign);
+        ::tsr::note_launch();
+        k_cone_x<EMPTINESS><<<x_grid, PT_BLOCK, 0, st>>>(nlinks, lrec.p, tr, recs.p, (float)t.root_size, esum, elen,
+                                                        accepted.p, next_link.p, accepted.p + 2, err.p, sign);
+        ::tsr::note_launch();
+    }
+    if (sign > 0.0) {
+        k_leaf_flags<<<grid_for(nl, BLK), BLK, 0, st>>>(nl, t.leaf_node.p, esum, o.states.p, FLAG_EMPTINESS);
+        ::tsr::note_launch();
+    }
     o.stage_ms[2] = timer.lap();
     o.prior.alloc(nl, st);
     DBuf<uint8_t> need;   // pruned field: leaves whose prior is queried
@@ -959,8 +1007,13 @@ void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_
         ::tsr::note_launch();
     }
     o.stage_ms[3] = timer.lap();
-    o.cone_count = read_scalar(cone_count.p, st);
-    o.e_sum.alloc(nl, st); o.s_sum.alloc(nl, st); o.e_len.alloc(nl, st); o.s_len.alloc(nl, st); o.occ.alloc(nl, st);
+    if (update) {
+        o.cone_count += read_scalar(cone_count.p, st);
+    } else {
+        o.cone_count = read_scalar(cone_count.p, st);
+        o.e_sum.alloc(nl, st); o.s_sum.alloc(nl, st); o.e_len.alloc(nl, st); o.s_len.alloc(nl, st);
+        o.occ.alloc(nl, st);
+    }
     k_finalize<<<grid_for(nl, BLK), BLK, 0, st>>>(nl, esum, ssum, elen, slen, o.prior.p, o.cone_count,
                                                  p.confidence_threshold, pred, need.p, o.e_sum.p, o.s_sum.p,
                                                  o.e_len.p, o.s_len.p, o.occ.p); ::tsr::note_launch();

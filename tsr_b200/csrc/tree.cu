@@ -983,6 +983,75 @@ struct EventTimer {
 }  // namespace
 
 // ====================================================================== API
+namespace {
+
+// ---- Tree::eraseSamples (Tree.cpp:50-53, Nodes.cpp:644-671) with
+// Samples::compact for the tree's own copy of the samples.
+// offsets[i] = erased samples before i (tree order), offsets[n] = total.
+__global__ void k_erase_nodes(uint32_t nn, const uint32_t *offsets, uint32_t *counts, uint32_t *starts) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nn) return;
+    const uint32_t start = starts[i], end = start + counts[i];
+    counts[i] -= offsets[end] - offsets[start];
+    starts[i] = start - offsets[start];
+}
+
+__global__ void k_compact_samples(uint32_t n, uint32_t k, const uint8_t *inliers, const uint32_t *offsets,
+                                  const D3 *pos, const D3 *nrm, const double *scale, const double *conf,
+                                  const uint32_t *links, D3 *o_pos, D3 *o_nrm, double *o_scale, double *o_conf,
+                                  uint32_t *o_links) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || !inliers[i]) return;
+    const uint32_t j = i - offsets[i];
+    o_pos[j] = pos[i];
+    o_nrm[j] = nrm[i];
+    o_scale[j] = scale[i];
+    o_conf[j] = conf[i];
+    for (uint32_t c = 0; c < k; ++c) o_links[(size_t)j * k + c] = links[(size_t)i * k + c];
+}
+
+// target[input index] = tree-order index, INVALID once erased
+__global__ void k_erase_targets(uint32_t n_in, const uint8_t *inliers, const uint32_t *offsets, uint32_t *target) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_in) return;
+    const uint32_t t = target[i];
+    if (t == INVALID) return;
+    target[i] = inliers[t] ? t - offsets[t] : INVALID;
+}
+
+__global__ void k_outlier_flags(uint32_t n, const uint8_t *inliers, uint32_t *flags) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i <= n) flags[i] = (i < n && !inliers[i]) ? 1u : 0u;
+}
+
+}  // namespace
+
+void erase_tree_samples(tsr_tree &t, const uint8_t *inliers) {
+    cudaStream_t st = t.stream;
+    const uint32_t n = t.n_samples, k = t.k, nn = t.n_nodes;
+    DBuf<uint32_t> flags(n + 1, st), offsets(n + 1, st);
+    k_outlier_flags<<<grid_for(n + 1, BLK), BLK, 0, st>>>(n, inliers, flags.p); ::tsr::note_launch();
+    exclusive_scan(flags.p, offsets.p, n + 1, st);
+    const uint32_t erased = read_scalar(offsets.p + n, st);
+    k_erase_nodes<<<grid_for(nn, BLK), BLK, 0, st>>>(nn, offsets.p, t.counts.p, t.starts.p); ::tsr::note_launch();
+    const uint32_t m = n - erased;
+    DBuf<D3> pos(m, st), nrm(m, st);
+    DBuf<double> scale(m, st), conf(m, st);
+    DBuf<uint32_t> links((size_t)m * k, st);
+    k_compact_samples<<<grid_for(n, BLK), BLK, 0, st>>>(n, k, inliers, offsets.p, t.pos.p, t.nrm.p, t.scale.p, t.conf.p,
+                                                        t.links.p, pos.p, nrm.p, scale.p, conf.p, links.p);
+    ::tsr::note_launch();
+    k_erase_targets<<<grid_for(t.target.n, BLK), BLK, 0, st>>>((uint32_t)t.target.n, inliers, offsets.p,
+                                                               t.target.p); ::tsr::note_launch();
+    t.pos = std::move(pos);
+    t.nrm = std::move(nrm);
+    t.scale = std::move(scale);
+    t.conf = std::move(conf);
+    t.links = std::move(links);
+    t.n_samples = m;
+    TSR_CUDA(cudaGetLastError());
+}
+
 void build_tree(tsr_tree &t, const tsr_samples_view &sv, bool on_device) {
     cudaStream_t st = t.stream;
     const uint32_t n = sv.count, k = sv.cams_per_sample;
