@@ -37,7 +37,7 @@ UNIT = "samples/s"
 L2_BYTES = 126 * 1024 * 1024
 # DRAM bytes per unit (per link for the cone passes, per leaf for the priors),
 # from the ncu capture summarised in profiles/occupancy_kernels_csg1m.md
-TRAFFIC_PER_UNIT = {"occ.sampleness": 159.9, "occ.emptiness": 161.4, "occ.priors": 220.9}
+TRAFFIC_PER_UNIT = {"occ.sampleness": 161.0, "occ.emptiness": 163.5, "occ.priors": 197.2}
 CPU_SAMPLE_N = 60_000
 
 
