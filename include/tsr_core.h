@@ -104,7 +104,8 @@ typedef struct {
     uint64_t visited_sampleness;       /* tree nodes tested against a cone, SAMPLENESS pass */
     uint64_t visited_emptiness;        /* ... EMPTINESS pass */
     uint64_t visited_priors;           /* tree nodes classified by the prior sphere queries */
-    uint64_t pruned_leaves;            /* leaves the learned pruner skipped (0 for the plain field) */
+    uint64_t pruned_leaves;            /* prior queries the pruned field skipped (0 for the plain field) */
+    uint64_t repaired_leaves;          /* skipped leaves queried after all: they bordered a sign change */
 } tsr_occupancy_counts;
 
 /* The learned pruner (north_star's MLP; no counterpart in the reference).
@@ -258,7 +259,9 @@ TSR_API tsr_status tsr_mlp_infer_bf16(const float *x, uint32_t n, const float *p
  * a sign change (or within `dilation` rings of face neighbours of one) or
  * whose sign it is not sure of; E == 0 or S == 0 fixes the sign without a
  * prior.  A skipped reliable leaf takes the pruner's sign, with the value
- * 0.5 (S - E) / coneCount when positive; its prior reads NaN. */
+ * 0.5 (S - E) / coneCount when positive; its prior reads NaN.  Skipped
+ * leaves that then border a leaf of the other sign are queried after all,
+ * until none does, so every leaf on a sign change has its exact value. */
 TSR_API tsr_status tsr_occupancy_compute_pruned(const tsr_tree *tree, const tsr_cameras_view *cameras,
                                                 const tsr_params *params, const tsr_pruner *pruner,
                                                 void *cuda_stream, tsr_occupancy **out_occupancy);

@@ -47,6 +47,7 @@ struct tsr_occupancy {
     uint64_t visits[3] = {0, 0, 0};  // nodes tested: EMPTINESS, SAMPLENESS, priors
     uint64_t links = 0;
     uint64_t pruned = 0;             // leaves whose prior query the pruned field skipped
+    uint64_t repaired = 0;           // skipped leaves queried after all (bordering a sign change)
 };
 
 struct tsr_mesh {

@@ -503,6 +503,28 @@ __global__ void __launch_bounds__(PT_BLOCK, (TYPE == 0) ? 6 : 5) k_cone_x(uint64
     }
 }
 
+// Pruned field repair: skipped reliable leaves (need == 0, E + S >= the
+// threshold) that border a leaf of the other sign.
+__global__ void k_repair_mark(uint32_t nl, const uint32_t *nb_off, const uint32_t *nbs, const double *occ,
+                              const uint8_t *need, const double *esum, const double *ssum, double threshold,
+                              uint8_t *mark) {
+    uint32_t l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= nl) return;
+    auto skipped = [&](uint32_t x) { return !need[x] && !((esum[x] + ssum[x]) < threshold); };
+    const bool pl = occ[l] > 0.0;
+    for (uint32_t e = nb_off[l]; e < nb_off[l + 1]; ++e) {
+        const uint32_t m = nbs[e];
+        if ((occ[m] > 0.0) == pl) continue;
+        if (skipped(l)) mark[l] = 1;
+        if (skipped(m)) mark[m] = 1;
+    }
+}
+
+__global__ void k_set_needed(uint32_t n, const uint32_t *list, uint8_t *need) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) need[list[i]] = 1;
+}
+
 __global__ void k_iota(uint32_t n, uint32_t *out) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) out[i] = i;
@@ -979,6 +1001,7 @@ void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_
         k_prior_needed<<<grid_for(nl, BLK), BLK, 0, st>>>(nl, pred, esum, ssum, p.confidence_threshold, need.p);
         ::tsr::note_launch();
     }
+    DBuf<double2> psum;   // cumulative prior sums (kept for the pruned field's repairs)
     {
         // the queried leaves: all of them, or the selected ones of a pruned field
         DBuf<uint32_t> list;
@@ -994,7 +1017,7 @@ void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_
             nq = read_scalar(nsel.p, st);
             o.pruned = nl - nq;
         }
-        DBuf<double2> psum((size_t)nn * PK, st);
+        psum.alloc((size_t)nn * PK, st);
         for (int d = (int)t.level_start.size() - 2; d >= 0; --d) {
             uint32_t lo = t.level_start[d], hi = t.level_start[d + 1];
             k_prior_sums<<<grid_for(hi - lo, BLK), BLK, 0, st>>>(lo, hi, nn, t.level_order.p, t.children.p,
@@ -1017,6 +1040,36 @@ void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_
     k_finalize<<<grid_for(nl, BLK), BLK, 0, st>>>(nl, esum, ssum, elen, slen, o.prior.p, o.cone_count,
                                                  p.confidence_threshold, pred, need.p, o.e_sum.p, o.s_sum.p,
                                                  o.e_len.p, o.s_len.p, o.occ.p); ::tsr::note_launch();
+    if (pred) {
+        // Repair: a skipped leaf that borders a sign change after all was
+        // predicted wrongly, or its value matters to the surface; query its
+        // prior and recompute it, until no skipped leaf borders a sign change.
+        DBuf<uint8_t> mark(nl, st);
+        DBuf<uint32_t> ids(nl, st), flist(nl, st), nsel(1, st);
+        k_iota<<<grid_for(nl, BLK), BLK, 0, st>>>(nl, ids.p); ::tsr::note_launch();
+        size_t tmp = 0;
+        TSR_CUDA(cub::DeviceSelect::Flagged(nullptr, tmp, ids.p, mark.p, flist.p, nsel.p, (int)nl, st));
+        DBuf<uint8_t> tb(tmp, st);
+        for (int round = 0; round < 64; ++round) {
+            mark.zero();
+            k_repair_mark<<<grid_for(nl, BLK), BLK, 0, st>>>(nl, t.nb_off.p, t.nbs.p, o.occ.p, need.p, esum, ssum,
+                                                            p.confidence_threshold, mark.p); ::tsr::note_launch();
+            TSR_CUDA(cub::DeviceSelect::Flagged(tb.p, tmp, ids.p, mark.p, flist.p, nsel.p, (int)nl, st));
+            const uint32_t nf = read_scalar(nsel.p, st);
+            if (nf == 0) break;
+            k_set_needed<<<grid_for(nf, BLK), BLK, 0, st>>>(nf, flist.p, need.p); ::tsr::note_launch();
+            next_link.zero();
+            k_priors_x<<<prior_grid, PT_BLOCK, 0, st>>>(nf, nn, flist.p, t.leaf_node.p, t.leaf_min.p, t.depth.p,
+                                                       t.nmin.p, recs.p, psum.p, t.root_size,
+                                                       p.relative_radius_for_priors, o.prior.p, next_link.p,
+                                                       accepted.p + 4, err.p); ::tsr::note_launch();
+            k_finalize<<<grid_for(nl, BLK), BLK, 0, st>>>(nl, esum, ssum, elen, slen, o.prior.p, o.cone_count,
+                                                         p.confidence_threshold, pred, need.p, o.e_sum.p, o.s_sum.p,
+                                                         o.e_len.p, o.s_len.p, o.occ.p); ::tsr::note_launch();
+            o.pruned -= nf;
+            o.repaired += nf;
+        }
+    }
     o.stage_ms[4] = timer.lap();
     unsigned long long a[5];
     TSR_CUDA(cudaMemcpyAsync(a, accepted.p, sizeof(a), cudaMemcpyDeviceToHost, st));

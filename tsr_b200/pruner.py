@@ -192,6 +192,7 @@ def judge(tree, cams, pruner, params=None, stream=None):
     return {
         "leaves": int(op.shape[0]),
         "pruned_leaves": pruned.counts["pruned_leaves"],
+        "repaired_leaves": pruned.counts["repaired_leaves"],
         "sign_agreement": float(np.mean((op > 0) == (oq > 0))),
         "case_agreement": float(np.mean(mesh_plain.cases == mesh_pruned.cases)),
         "triangles": [int(mesh_plain.triangles.shape[0]), int(mesh_pruned.triangles.shape[0])],
