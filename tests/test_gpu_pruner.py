@@ -11,7 +11,7 @@ pytestmark = pytest.mark.gpu
 
 MIN_CASE_AGREEMENT = 0.999        # DMC case codes equal to the plain field's
 MAX_HAUSDORFF_LEAVES = 0.1        # vertex Hausdorff distance, in finest leaf sizes
-MIN_PRIOR_WORK_SAVED = 0.25       # fraction of prior-query node visits removed
+MIN_PRIOR_WORK_SAVED = 0.15       # fraction of prior-query node visits removed
 
 
 @pytest.fixture(scope="module")
