@@ -228,6 +228,44 @@ TSR_API tsr_status tsr_mesh_get_counts(const tsr_mesh *mesh, tsr_mesh_counts *ou
 TSR_API tsr_status tsr_mesh_copy(const tsr_mesh *mesh, uint8_t *cases, double *positions, double *scales,
                          uint32_t *edge_keys, uint32_t *triangles);
 
+/* What tsr_mesh_postprocess did. */
+typedef struct {
+    uint64_t isle_vertices, isle_triangles;   /* deleted with isles below the minimum size */
+    uint64_t border_edges;                    /* hole border edges after the isle deletion */
+    uint64_t holes;                           /* rings filled */
+    uint64_t hole_vertices, hole_triangles;   /* added by the filling */
+    uint64_t skipped_rings;                   /* rings of < 3 edges, left open */
+} tsr_mesh_post_counts;
+
+/* The post-processing DualMarchingCells::DualMarchingCells runs after
+ * extractMesh (DualMarchingCells.cpp:26-39), in place on the mesh's stream:
+ *   FlexibleMesh::deleteIsolatedGeometry(min_isle_size) (FlexibleMesh.cpp:
+ *   1411-1426, IslesEraser.cpp): isles (vertices connected by edges) of fewer
+ *   than min_isle_size vertices are deleted and the rest compacted in order;
+ *   then, unless nothing is left, FlexibleMesh::fillHoles (FlexibleMesh.cpp:
+ *   1580-1931) and Mesh::computeNormalsWeightedByAngles (Mesh.cpp:145-203).
+ * The reference passes Scene::minimumTriangleIsleSize (App.cfg: 1000).
+ * Border edges are chained in the order one thread of the reference finds
+ * them (its OpenMP loop makes that order timing dependent).  Vertices the
+ * filling adds get scale 0 and edge keys {0xFFFFFFFF, 0xFFFFFFFF}; dual-cell
+ * cases are unchanged.  An edge shared by three or more triangles returns
+ * TSR_ERR_STATE and leaves the mesh unchanged (the reference throws,
+ * FlexibleMesh.cpp:1227-1259).  counts may be NULL. */
+TSR_API tsr_status tsr_mesh_postprocess(tsr_mesh *mesh, uint32_t min_isle_size, tsr_mesh_post_counts *counts);
+
+/* Vertex normals after tsr_mesh_postprocess, 3 doubles per vertex, HOST
+ * memory (zeros when post-processing left no triangles). */
+TSR_API tsr_status tsr_mesh_copy_normals(const tsr_mesh *mesh, double *normals);
+
+/* A mesh from HOST arrays, for tsr_mesh_postprocess of a surface that did
+ * not come from tsr_dmc_extract (FlexibleMesh's vertex and index arrays,
+ * FlexibleMesh.cpp:1276-1281, 1573-1578).  scales may be NULL (zeros); the
+ * mesh has no dual cells and its edge keys are 0xFFFFFFFF.  Triangle
+ * indices must be below the vertex count. */
+TSR_API tsr_status tsr_mesh_create(const double *positions, const double *scales, uint64_t vertex_count,
+                                   const uint32_t *triangles, uint64_t triangle_count, void *cuda_stream,
+                                   tsr_mesh **out_mesh);
+
 /* ---- learned pruner (no counterpart in the reference) ---- */
 /* The pruner's per-leaf features of a field, leaves x TSR_MLP_FEATURES floats
  * into HOST memory: log1p(samples in the leaf), log(mean sample scale / leaf
@@ -274,6 +312,56 @@ TSR_API unsigned long long tsr_kernel_launches(void);
  * this handle, per stage (see tsr_stage names in the implementation). */
 TSR_API tsr_status tsr_tree_stage_ms(const tsr_tree *tree, float *ms, int n);
 TSR_API tsr_status tsr_occupancy_stage_ms(const tsr_occupancy *occ, float *ms, int n);
+
+/* ---------------------------------------------------------------- files
+ * The reference's on-disk bodies, little endian, Real = double:
+ *   <prefix>.nodes      Nodes::saveToFile (Nodes.cpp:789-807)
+ *   <prefix>.leaves     Leaves::saveToFile (Leaves.cpp:261-292)
+ *   <prefix>.dualCells  DualCells::saveToFile (DualCells.cpp:378-385)
+ *   <path>              Occupancy::saveToFile (Occupancy.cpp:722-766)
+ *   <path>              Samples::saveToFile (Samples.cpp:733-765)
+ * Each file starts with a 16-byte header in place of the reference's
+ * BaseProject File header (that library is not part of the reference tree):
+ * "TSRF", u32 format 1, u32 FILE_VERSION 0, u32 kind (1 nodes, 2 leaves,
+ * 3 dual cells, 4 occupancy, 5 samples). */
+
+/* Tree::saveToFiles (Tree.cpp:129-134): writes the three tree files. */
+TSR_API tsr_status tsr_tree_save(const tsr_tree *tree, const char *path_prefix);
+
+/* Samples::saveToFile(beginning, false, true) (Samples.cpp:733-765): the
+ * tree's samples in tree order, <path> = <beginning>.samples, with the AABB
+ * the tree was built over (kept through tsr_tree_erase_samples, so that the
+ * file reloads the same tree).  colors: HOST, 3 per sample in tree order,
+ * or NULL for zeros (colours are not part of tsr_samples_view). */
+TSR_API tsr_status tsr_tree_save_samples(const tsr_tree *tree, const double *colors, const char *path);
+
+/* Tree::Tree(filesBeginning) / Tree::loadFromFile (Tree.cpp:39-43, 118-127):
+ * reads the three tree files.  The reference takes the samples and their
+ * AABB (Samples::mAABBWS, stored in the .samples file) from the Scene
+ * singleton; here the caller passes the samples, in tree order (as a
+ * .samples file or tsr_tree_copy_samples gives them), host memory, and
+ * optionally the AABB {min x, y, z, max x, y, z} of the samples file.  With
+ * aabb NULL it is computed from the samples exactly as tsr_tree_build does.
+ * The root scope follows from the AABB as in Tree::getRootScope
+ * (Tree.cpp:70-101), and every saved leaf scope must equal the one it gives,
+ * bit for bit.  A file of another tree or of other samples, a damaged file
+ * and any index out of range return TSR_ERR_INVALID_ARG before any device
+ * work (the reference throws FileCorruptionException).  The loaded tree's
+ * permutation is the identity. */
+TSR_API tsr_status tsr_tree_load(const char *path_prefix, const tsr_samples_view *samples, const double *aabb,
+                                 const tsr_params *params, void *cuda_stream, tsr_tree **out_tree);
+
+/* Occupancy::saveToFile (Occupancy.cpp:722-766).  A pruned field with
+ * skipped prior queries returns TSR_ERR_STATE: the format holds a prior for
+ * every leaf. */
+TSR_API tsr_status tsr_occupancy_save(const tsr_occupancy *occ, const char *path);
+
+/* Occupancy::Occupancy(fileName) / loadFromFile (Occupancy.cpp:598-603,
+ * 663-720): reads sums, cone lengths, priors, node states and cone count
+ * for `tree` (counts must match) and computes the occupancy of every leaf
+ * with params->confidence_threshold (NULL: the tree's parameters). */
+TSR_API tsr_status tsr_occupancy_load(const tsr_tree *tree, const char *path, const tsr_params *params,
+                                      void *cuda_stream, tsr_occupancy **out_occupancy);
 
 #ifdef __cplusplus
 }

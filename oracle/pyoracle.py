@@ -49,6 +49,11 @@ def lib():
         L.tsro_get_mesh.argtypes = [P, P, P, P, P, P]
         L.tsro_stage_seconds.restype = ctypes.c_double
         L.tsro_stage_seconds.argtypes = [P, ctypes.c_int]
+        L.tsro_mesh_postprocess.restype = P
+        L.tsro_mesh_postprocess.argtypes = [ctypes.c_uint32, P, P, ctypes.c_uint32, P, ctypes.c_uint32]
+        L.tsro_mesh_free.argtypes = [P]
+        L.tsro_mesh_counts.argtypes = [P, P]
+        L.tsro_mesh_get.argtypes = [P, P, P, P, P]
         _lib = L
     return _lib
 
@@ -167,3 +172,28 @@ class Oracle:
         names = ["containment", "sampling", "balance", "reorder", "leaves", "dual_cells",
                  "sampleness", "emptiness", "priors", "dmc"]
         return {n: lib().tsro_stage_seconds(self.h, i) for i, n in enumerate(names)}
+
+
+MESH_COUNT_KEYS = ("vertices", "triangles", "error", "isle_vertices", "isle_triangles", "border_edges", "holes",
+                   "hole_vertices", "hole_triangles", "skipped_rings")
+
+
+def mesh_postprocess(positions, triangles, scales=None, min_isle_size=1000):
+    """The post-processing of DualMarchingCells (isles, holes, normals) on
+    the CPU; returns (counts, positions, normals, scales, triangles)."""
+    L = lib()
+    pos = np.ascontiguousarray(positions, np.float64).reshape(-1, 3)
+    tri = np.ascontiguousarray(triangles, np.uint32).reshape(-1, 3)
+    sc = None if scales is None else np.ascontiguousarray(scales, np.float64)
+    h = L.tsro_mesh_postprocess(pos.shape[0], _p(pos), _p(sc), tri.shape[0], _p(tri), min_isle_size)
+    try:
+        c = np.zeros(len(MESH_COUNT_KEYS), np.uint64)
+        L.tsro_mesh_counts(h, _p(c))
+        counts = {k: int(v) for k, v in zip(MESH_COUNT_KEYS, c)}
+        nv, nt = counts["vertices"], counts["triangles"]
+        p, n, s = np.zeros((nv, 3)), np.zeros((nv, 3)), np.zeros(nv)
+        t = np.zeros((nt, 3), np.uint32)
+        L.tsro_mesh_get(h, _p(p), _p(n), _p(s), _p(t))
+    finally:
+        L.tsro_mesh_free(h)
+    return counts, p, n, s, t

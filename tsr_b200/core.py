@@ -17,6 +17,7 @@ Failures raise ``TsrError`` (the reference throws FailureHandling::Exception).
 from __future__ import annotations
 
 import ctypes
+import os
 from pathlib import Path
 
 import numpy as np
@@ -66,6 +67,12 @@ class tsr_occupancy_counts(ctypes.Structure):
 MLP_FEATURES, MLP_HIDDEN, MLP_OUTPUTS, MLP_PARAMS = 10, 64, 2, 4994
 
 
+class tsr_mesh_post_counts(ctypes.Structure):
+    _fields_ = [("isle_vertices", ctypes.c_uint64), ("isle_triangles", ctypes.c_uint64),
+                ("border_edges", ctypes.c_uint64), ("holes", ctypes.c_uint64), ("hole_vertices", ctypes.c_uint64),
+                ("hole_triangles", ctypes.c_uint64), ("skipped_rings", ctypes.c_uint64)]
+
+
 class tsr_pruner(ctypes.Structure):
     _fields_ = [("weights", _P), ("feature_mean", ctypes.c_float * MLP_FEATURES),
                 ("feature_inv_std", ctypes.c_float * MLP_FEATURES), ("sign_threshold", ctypes.c_float),
@@ -108,6 +115,14 @@ _sig = {
     "tsr_mlp_forward": (ctypes.c_int, [_P, ctypes.c_uint32, _P, _P, _P]),
     "tsr_mlp_infer_bf16": (ctypes.c_int, [_P, ctypes.c_uint32, _P, _P, _P]),
     "tsr_occupancy_compute_pruned": (ctypes.c_int, [_P, _P, _P, _P, _P, _P]),
+    "tsr_mesh_postprocess": (ctypes.c_int, [_P, ctypes.c_uint32, _P]),
+    "tsr_mesh_copy_normals": (ctypes.c_int, [_P, _P]),
+    "tsr_mesh_create": (ctypes.c_int, [_P, _P, ctypes.c_uint64, _P, ctypes.c_uint64, _P, _P]),
+    "tsr_tree_save": (ctypes.c_int, [_P, ctypes.c_char_p]),
+    "tsr_tree_save_samples": (ctypes.c_int, [_P, _P, ctypes.c_char_p]),
+    "tsr_tree_load": (ctypes.c_int, [ctypes.c_char_p, _P, _P, _P, _P, _P]),
+    "tsr_occupancy_save": (ctypes.c_int, [_P, ctypes.c_char_p]),
+    "tsr_occupancy_load": (ctypes.c_int, [_P, ctypes.c_char_p, _P, _P, _P]),
 }
 for _name, (_res, _args) in _sig.items():
     _f = getattr(lib, _name)
@@ -270,18 +285,54 @@ class Tree:
         v = samples.view()
         _check(lib.tsr_tree_build(ctypes.byref(v), ctypes.byref(self.params), _stream_ptr(stream),
                                   ctypes.byref(self._h)))
-        c = tsr_tree_counts()
-        _check(lib.tsr_tree_get_counts(self._h, ctypes.byref(c)))
-        self.counts = {k: int(getattr(c, k)) for k, _ in tsr_tree_counts._fields_}
-        self.sample_count = samples.count
-        self.input_count = samples.count
+        self._read_counts(samples.count)
         if reorder_samples:
             # the reference reorders Samples in place (Nodes.cpp:630); copy the
             # device-side reordered arrays back instead of permuting on the host
             _check(lib.tsr_tree_copy_samples(self._h, _ptr(samples.positions), _ptr(samples.normals),
                                              _ptr(samples.scales), _ptr(samples.confidences),
                                              _ptr(samples.camera_links)))
+
+    def _read_counts(self, sample_count):
+        c = tsr_tree_counts()
+        _check(lib.tsr_tree_get_counts(self._h, ctypes.byref(c)))
+        self.counts = {k: int(getattr(c, k)) for k, _ in tsr_tree_counts._fields_}
+        self.sample_count = sample_count
+        self.input_count = sample_count
         self._nodes = self._leaves = self._cells = None
+
+    @classmethod
+    def fromFiles(cls, prefix, samples: Samples, aabb=None, params=None, stream=None):
+        """Tree::Tree(filesBeginning) (Tree.cpp:39-43): the tree of
+        ``prefix``.nodes / .leaves / .dualCells over ``samples`` in tree
+        order (the order a built tree leaves them in).  ``aabb``: the
+        samples file's AABB (min xyz, max xyz); None computes it from the
+        samples."""
+        self = cls.__new__(cls)
+        self._h = _P()
+        self.params = params or params_default()
+        self._stream = stream
+        v = samples.view()
+        bb = None if aabb is None else np.ascontiguousarray(aabb, np.float64).reshape(-1)
+        if bb is not None and bb.shape != (6,):
+            raise ValueError("AABB: min x, y, z and max x, y, z")
+        _check(lib.tsr_tree_load(os.fsencode(prefix), ctypes.byref(v), _ptr(bb) if bb is not None else None,
+                                 ctypes.byref(self.params), _stream_ptr(stream), ctypes.byref(self._h)))
+        self._read_counts(samples.count)
+        return self
+
+    def saveToFiles(self, prefix):
+        """Tree::saveToFiles (Tree.cpp:129-134)."""
+        _check(lib.tsr_tree_save(self._h, os.fsencode(prefix)))
+
+    def saveSamples(self, path, colors=None):
+        """Samples::saveToFile (Samples.cpp:733-765) of the tree's samples in
+        tree order with the AABB the tree was built over; ``colors``: 3 per
+        sample in tree order, or None for zeros."""
+        c = None if colors is None else np.ascontiguousarray(colors, np.float64)
+        if c is not None and c.shape != (self.sample_count, 3):
+            raise ValueError("one RGB colour per sample expected")
+        _check(lib.tsr_tree_save_samples(self._h, _ptr(c) if c is not None else None, os.fsencode(path)))
 
     def __del__(self):
         if getattr(self, "_h", None) and self._h:
@@ -379,12 +430,31 @@ class Occupancy:
             pv = pruner.view()
             _check(lib.tsr_occupancy_compute_pruned(tree.handle, ctypes.byref(cameras.view()), ctypes.byref(p),
                                                     ctypes.byref(pv), _stream_ptr(stream), ctypes.byref(self._h)))
+        self._created(stream)
+
+    def _created(self, stream):
         c = tsr_occupancy_counts()
         _check(lib.tsr_occupancy_get_counts(self._h, ctypes.byref(c)))
         self.counts = {k: int(getattr(c, k)) for k, _ in tsr_occupancy_counts._fields_}
         self._cache = {}
         self.mCrust = None
         self._stream = stream
+
+    @classmethod
+    def fromFile(cls, tree: Tree, path, params=None, stream=None):
+        """Occupancy::Occupancy(fileName) (Occupancy.cpp:598-602) for ``tree``."""
+        self = cls.__new__(cls)
+        self._h = _P()
+        self.tree = tree
+        p = params or tree.params
+        _check(lib.tsr_occupancy_load(tree.handle, os.fsencode(path), ctypes.byref(p), _stream_ptr(stream),
+                                      ctypes.byref(self._h)))
+        self._created(stream)
+        return self
+
+    def saveToFile(self, path):
+        """Occupancy::saveToFile (Occupancy.cpp:722-766)."""
+        _check(lib.tsr_occupancy_save(self._h, os.fsencode(path)))
 
     def __del__(self):
         if getattr(self, "_h", None) and self._h:
@@ -461,10 +531,12 @@ class Occupancy:
         v = self.field("sampleness_sum") / self.field("cone_count")
         return v if leaf is None else float(v[leaf])
 
-    def extractCrust(self, stream=None):
-        """Occupancy::extractCrust (Occupancy.cpp:523-528) without the
-        FlexibleMesh post-processing."""
-        self.mCrust = DualMarchingCells(self, stream=stream if stream is not None else self._stream)
+    def extractCrust(self, stream=None, min_isle_size=None):
+        """Occupancy::extractCrust (Occupancy.cpp:523-528); the FlexibleMesh
+        post-processing runs when ``min_isle_size`` is given (the reference
+        always runs it, with Scene::minimumTriangleIsleSize = 1000)."""
+        self.mCrust = DualMarchingCells(self, stream=stream if stream is not None else self._stream,
+                                        min_isle_size=min_isle_size)
         return self.mCrust
 
     def getCrust(self):
@@ -472,24 +544,69 @@ class Occupancy:
 
 
 class DualMarchingCells:
-    """DualMarchingCells::extractMesh (DualMarchingCells.cpp:41-169)."""
+    """DualMarchingCells (DualMarchingCells.cpp:26-169): extractMesh, and
+    with ``min_isle_size`` the post-processing of its constructor
+    (deleteIsolatedGeometry, fillHoles, computeNormalsWeightedByAngles) on
+    the GPU too; the reference passes Scene::minimumTriangleIsleSize = 1000."""
 
-    def __init__(self, occupancy: Occupancy, stream=None):
+    def __init__(self, occupancy: Occupancy, stream=None, min_isle_size=None):
         self._h = _P()
         _check(lib.tsr_dmc_extract(occupancy.tree.handle, occupancy.handle, _stream_ptr(stream),
                                    ctypes.byref(self._h)))
+        self.n_cells = occupancy.tree.counts["dual_cells"]
+        self.post_counts = None
+        if min_isle_size is not None:
+            self._postprocess(min_isle_size)
+        self._read()
+
+    @classmethod
+    def fromArrays(cls, positions, triangles, scales=None, stream=None, min_isle_size=None):
+        """A FlexibleMesh of the given vertices and triangles (for the
+        post-processing of a surface from elsewhere)."""
+        self = cls.__new__(cls)
+        self._h = _P()
+        pos = np.ascontiguousarray(positions, np.float64).reshape(-1, 3)
+        tri = np.ascontiguousarray(triangles, np.uint32).reshape(-1, 3)
+        sc = None if scales is None else np.ascontiguousarray(scales, np.float64).reshape(-1)
+        if sc is not None and sc.shape[0] != pos.shape[0]:
+            raise ValueError("one scale per vertex expected")
+        _check(lib.tsr_mesh_create(_ptr(pos), _ptr(sc) if sc is not None else None, pos.shape[0], _ptr(tri),
+                                   tri.shape[0], _stream_ptr(stream), ctypes.byref(self._h)))
+        self.n_cells = 0
+        self.post_counts = None
+        if min_isle_size is not None:
+            self._postprocess(min_isle_size)
+        self._read()
+        return self
+
+    def _postprocess(self, min_isle_size):
+        pc = tsr_mesh_post_counts()
+        _check(lib.tsr_mesh_postprocess(self._h, int(min_isle_size), ctypes.byref(pc)))
+        self.post_counts = {k: int(getattr(pc, k)) for k, _ in tsr_mesh_post_counts._fields_}
+
+    def postprocess(self, min_isle_size=1000):
+        """The reference constructor's post-processing (DualMarchingCells.cpp:31-36)."""
+        self._postprocess(min_isle_size)
+        self._read()
+        return self.post_counts
+
+    def _read(self):
         c = tsr_mesh_counts()
         _check(lib.tsr_mesh_get_counts(self._h, ctypes.byref(c)))
         self.counts = {k: int(getattr(c, k)) for k, _ in tsr_mesh_counts._fields_}
-        nc = occupancy.tree.counts["dual_cells"]
         nv, nt = self.counts["vertices"], self.counts["triangles"]
-        self.cases = np.zeros(nc, np.uint8)
+        self.cases = np.zeros(self.n_cells, np.uint8)
         self.positions = np.zeros((nv, 3))
         self.scales = np.zeros(nv)
         self.edge_keys = np.zeros((nv, 2), np.uint32)
         self.triangles = np.zeros((nt, 3), np.uint32)
-        _check(lib.tsr_mesh_copy(self._h, _ptr(self.cases), _ptr(self.positions), _ptr(self.scales),
-                                 _ptr(self.edge_keys), _ptr(self.triangles)))
+        _check(lib.tsr_mesh_copy(self._h, _ptr(self.cases) if self.n_cells else None, _ptr(self.positions),
+                                 _ptr(self.scales), _ptr(self.edge_keys), _ptr(self.triangles)))
+        self.normals = None
+        if self.post_counts is not None:
+            self.normals = np.zeros((nv, 3))
+            if nv:
+                _check(lib.tsr_mesh_copy_normals(self._h, _ptr(self.normals)))
 
     def __del__(self):
         if getattr(self, "_h", None) and self._h:

@@ -120,22 +120,25 @@ const char *tsr_last_error_message(void) { return g_last_error.c_str(); }
 
 const char *tsr_version(void) { return "tsr_b200 core 0.1 (sm_100a)"; }
 
+static void check_samples(const tsr_samples_view &sv, bool on_device) {
+    if (sv.count == 0) fail(TSR_ERR_INVALID_ARG, "no samples to build a tree from (Scene.cpp:141-146)");
+    if (sv.cams_per_sample == 0) fail(TSR_ERR_INVALID_ARG, "cams_per_sample must be >= 1");
+    if (!sv.positions || !sv.normals || !sv.scales || !sv.confidences || !sv.camera_links)
+        fail(TSR_ERR_INVALID_ARG, "null sample array");
+    if ((uint64_t)sv.count * sv.cams_per_sample >= 0xFFFFFFFFull)
+        fail(TSR_ERR_OVERFLOW_U32, "link count must stay below 2^32 - 1 (Samples.h:395-402)");
+    if (!on_device)
+        for (uint32_t i = 0; i < sv.count; ++i)
+            if (!(sv.scales[i] > 0.0))   // Samples.cpp:280-288
+                fail(TSR_ERR_INVALID_ARG, "invalid (non-positive) sample scale at index " + std::to_string(i));
+}
+
 static tsr_status tree_build_impl(const tsr_samples_view *samples, const tsr_params *params, void *cuda_stream,
                                   tsr_tree **out_tree, bool on_device) {
     if (out_tree) *out_tree = nullptr;
     return guarded([&] {
         if (!samples || !out_tree) fail(TSR_ERR_INVALID_ARG, "null argument");
-        if (samples->count == 0) fail(TSR_ERR_INVALID_ARG, "no samples to build a tree from (Scene.cpp:141-146)");
-        if (samples->cams_per_sample == 0) fail(TSR_ERR_INVALID_ARG, "cams_per_sample must be >= 1");
-        if (!samples->positions || !samples->normals || !samples->scales || !samples->confidences ||
-            !samples->camera_links)
-            fail(TSR_ERR_INVALID_ARG, "null sample array");
-        if ((uint64_t)samples->count * samples->cams_per_sample >= 0xFFFFFFFFull)
-            fail(TSR_ERR_OVERFLOW_U32, "link count must stay below 2^32 - 1 (Samples.h:395-402)");
-        if (!on_device)
-            for (uint32_t i = 0; i < samples->count; ++i)
-                if (!(samples->scales[i] > 0.0))   // Samples.cpp:280-288
-                    fail(TSR_ERR_INVALID_ARG, "invalid (non-positive) sample scale at index " + std::to_string(i));
+        check_samples(*samples, on_device);
         tsr_params p;
         tsr_params_default(&p);
         if (params) p = *params;
@@ -489,6 +492,129 @@ tsr_status tsr_mesh_copy(const tsr_mesh *m, uint8_t *cases, double *positions, d
         to_host(m->vkeys, 2 * m->n_verts, edge_keys, m->stream);
         to_host(m->tris, 3 * m->n_tris, triangles, m->stream);
         TSR_CUDA(cudaStreamSynchronize(m->stream));
+    });
+}
+
+tsr_status tsr_mesh_postprocess(tsr_mesh *m, uint32_t min_isle_size, tsr_mesh_post_counts *counts) {
+    return guarded([&] {
+        if (!m) fail(TSR_ERR_INVALID_ARG, "null mesh");
+        tsr_mesh_post_counts pc{};
+        postprocess_mesh(*m, min_isle_size, pc);
+        if (counts) *counts = pc;
+    });
+}
+
+tsr_status tsr_mesh_copy_normals(const tsr_mesh *m, double *normals) {
+    return guarded([&] {
+        if (!m || !normals) fail(TSR_ERR_INVALID_ARG, "null argument");
+        if (m->vnrm.n != 3 * m->n_verts) fail(TSR_ERR_STATE, "normals exist after tsr_mesh_postprocess only");
+        to_host(m->vnrm, 3 * m->n_verts, normals, m->stream);
+        TSR_CUDA(cudaStreamSynchronize(m->stream));
+    });
+}
+
+tsr_status tsr_mesh_create(const double *positions, const double *scales, uint64_t vertex_count,
+                           const uint32_t *triangles, uint64_t triangle_count, void *cuda_stream, tsr_mesh **out) {
+    if (out) *out = nullptr;
+    return guarded([&] {
+        if (!out || (vertex_count && !positions) || (triangle_count && !triangles))
+            fail(TSR_ERR_INVALID_ARG, "null argument");
+        if (vertex_count >= INVALID || 3 * triangle_count >= INVALID)
+            fail(TSR_ERR_OVERFLOW_U32, "vertex and corner counts must stay below 2^32 - 1");
+        for (uint64_t i = 0; i < 3 * triangle_count; ++i)
+            if (triangles[i] >= vertex_count)
+                fail(TSR_ERR_INVALID_ARG, "triangle index out of range at corner " + std::to_string(i));
+        tsr_mesh *m = new tsr_mesh();
+        m->stream = (cudaStream_t)cuda_stream;
+        try {
+            cudaStream_t st = m->stream;
+            m->n_verts = vertex_count;
+            m->n_tris = triangle_count;
+            m->vpos.alloc(3 * vertex_count, st);
+            m->vscale.alloc(vertex_count, st);
+            m->vkeys.alloc(2 * vertex_count, st);
+            m->tris.alloc(3 * triangle_count, st);
+            if (vertex_count) {
+                TSR_CUDA(cudaMemcpyAsync(m->vpos.p, positions, 24 * vertex_count, cudaMemcpyHostToDevice, st));
+                if (scales) TSR_CUDA(cudaMemcpyAsync(m->vscale.p, scales, 8 * vertex_count, cudaMemcpyHostToDevice, st));
+                else m->vscale.zero();
+                m->vkeys.fill_bytes(0xFF);
+            }
+            if (triangle_count)
+                TSR_CUDA(cudaMemcpyAsync(m->tris.p, triangles, 12 * triangle_count, cudaMemcpyHostToDevice, st));
+            TSR_CUDA(cudaStreamSynchronize(st));
+        } catch (...) {
+            delete m;
+            throw;
+        }
+        *out = m;
+    });
+}
+
+tsr_status tsr_tree_save(const tsr_tree *tree, const char *path_prefix) {
+    return guarded([&] {
+        if (!tree || !path_prefix || !*path_prefix) fail(TSR_ERR_INVALID_ARG, "null argument");
+        save_tree(*tree, path_prefix);
+    });
+}
+
+tsr_status tsr_tree_save_samples(const tsr_tree *tree, const double *colors, const char *path) {
+    return guarded([&] {
+        if (!tree || !path || !*path) fail(TSR_ERR_INVALID_ARG, "null argument");
+        save_samples(*tree, colors, path);
+    });
+}
+
+tsr_status tsr_tree_load(const char *path_prefix, const tsr_samples_view *samples, const double *aabb,
+                         const tsr_params *params, void *cuda_stream, tsr_tree **out_tree) {
+    if (out_tree) *out_tree = nullptr;
+    return guarded([&] {
+        if (!path_prefix || !*path_prefix || !samples || !out_tree) fail(TSR_ERR_INVALID_ARG, "null argument");
+        check_samples(*samples, false);
+        tsr_params p;
+        tsr_params_default(&p);
+        if (params) p = *params;
+        check_params(p);
+        tsr_tree *t = new tsr_tree();
+        t->stream = (cudaStream_t)cuda_stream;
+        t->params = p;
+        try {
+            load_tree(*t, path_prefix, *samples, aabb);
+        } catch (...) {
+            delete t;
+            throw;
+        }
+        *out_tree = t;
+    });
+}
+
+tsr_status tsr_occupancy_save(const tsr_occupancy *occ, const char *path) {
+    return guarded([&] {
+        if (!occ || !path || !*path) fail(TSR_ERR_INVALID_ARG, "null argument");
+        if (occ->pruned)
+            fail(TSR_ERR_STATE, "a pruned field holds no prior for its skipped leaves; the file format needs all");
+        save_occupancy(*occ, path);
+    });
+}
+
+tsr_status tsr_occupancy_load(const tsr_tree *tree, const char *path, const tsr_params *params, void *cuda_stream,
+                              tsr_occupancy **out) {
+    if (out) *out = nullptr;
+    return guarded([&] {
+        if (!tree || !path || !*path || !out) fail(TSR_ERR_INVALID_ARG, "null argument");
+        if (tree->n_leaves == 0) fail(TSR_ERR_STATE, "tree has no leaves");
+        tsr_params p = tree->params;
+        if (params) p = *params;
+        check_params(p);
+        tsr_occupancy *o = new tsr_occupancy();
+        o->stream = (cudaStream_t)cuda_stream;
+        try {
+            load_occupancy(*tree, *o, path, p);
+        } catch (...) {
+            delete o;
+            throw;
+        }
+        *out = o;
     });
 }
 

@@ -9,6 +9,7 @@ struct tsr_tree {
     cudaStream_t stream = nullptr;
     tsr_params params{};
     uint32_t n_samples = 0, k = 0;
+    double aabb[6] = {0, 0, 0, 0, 0, 0};   // Samples::mAABBWS at the build: min xyz, max xyz
     double root_min[3] = {0, 0, 0};
     double root_size = 0;
     uint32_t n_nodes = 0, n_leaves = 0, max_depth = 0, n_cells = 0;
@@ -56,6 +57,7 @@ struct tsr_mesh {
     tsr::DBuf<uint8_t> cases;
     tsr::DBuf<double> vpos, vscale;
     tsr::DBuf<uint32_t> vkeys, tris;
+    tsr::DBuf<double> vnrm;            // 3 per vertex once post-processed; empty before
 };
 
 namespace tsr {
@@ -75,7 +77,15 @@ void mlp_infer_bf16(const float *x, uint32_t n, const float *params, float *out,
 void pruner_predict(const tsr_tree &t, const tsr_pruner &pr, const double *esum, const double *ssum,
                     double threshold, DBuf<uint8_t> &pred, cudaStream_t st);
 void extract_dmc(const tsr_tree &t, const tsr_occupancy &o, tsr_mesh &m);
+void postprocess_mesh(tsr_mesh &m, uint32_t min_isle_size, tsr_mesh_post_counts &counts);
 void reserve_pool(size_t want, cudaStream_t st);
 void root_scope_noalloc(uint64_t count, const double *positions, const double *scales, double h_svo,
                         double *out_min_xyz_size, cudaStream_t st);
+void finalize_field(tsr_occupancy &o, const tsr_params &p);
+void save_tree(const tsr_tree &t, const std::string &prefix);
+void root_from_aabb(tsr_tree &t);
+void load_tree(tsr_tree &t, const std::string &prefix, const tsr_samples_view &sv, const double *aabb);
+void save_samples(const tsr_tree &t, const double *colors, const std::string &path);
+void save_occupancy(const tsr_occupancy &o, const std::string &path);
+void load_occupancy(const tsr_tree &t, tsr_occupancy &o, const std::string &path, const tsr_params &p);
 }  // namespace tsr

@@ -1084,4 +1084,18 @@ void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_
     TSR_CUDA(cudaGetLastError());
 }
 
+// The occupancy of every leaf from sums, cone lengths, priors and cone count
+// already in the field's buffers (a field read from a file): the plain
+// formula of k_finalize, sums copied onto themselves.
+void finalize_field(tsr_occupancy &o, const tsr_params &p) {
+    const uint32_t nl = o.n_leaves;
+    o.occ.alloc(nl, o.stream);
+    if (!nl) return;
+    k_finalize<<<grid_for(nl, BLK), BLK, 0, o.stream>>>(nl, o.e_sum.p, o.s_sum.p, o.e_len.p, o.s_len.p, o.prior.p,
+                                                       o.cone_count, p.confidence_threshold, nullptr, nullptr,
+                                                       o.e_sum.p, o.s_sum.p, o.e_len.p, o.s_len.p, o.occ.p);
+    ::tsr::note_launch();
+    TSR_CUDA(cudaGetLastError());
+}
+
 }  // namespace tsr

@@ -1088,11 +1088,11 @@ void build_tree(tsr_tree &t, const tsr_samples_view &sv, bool on_device) {
                 lo[j] = std::min(lo[j], h[b * 6 + j]);
                 hi[j] = std::max(hi[j], h[b * 6 + 3 + j]);
             }
-        double ext[3] = {hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]};
-        double size = std::max(std::max(ext[0], ext[1]), ext[2]);
-        double half = size * 0.5;
-        for (int j = 0; j < 3; ++j) t.root_min[j] = (lo[j] + hi[j]) * 0.5 - half;
-        t.root_size = size;
+        for (int j = 0; j < 3; ++j) {
+            t.aabb[j] = lo[j];
+            t.aabb[3 + j] = hi[j];
+        }
+        root_from_aabb(t);
     }
     Root root{D3{t.root_min[0], t.root_min[1], t.root_min[2]}, t.root_size};
 
