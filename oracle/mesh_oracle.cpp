@@ -408,6 +408,20 @@ tsro_mesh *tsro_mesh_postprocess(uint32_t nv, const double *positions, const dou
 
 void tsro_mesh_free(tsro_mesh *h) { delete h; }
 
+// The ring search alone: nb border edges (tail, head pairs in list order)
+// into rings of tail vertices; returns the ring count.  ring_verts holds nb
+// entries, ring_lens one per ring (at most nb).
+uint32_t tsro_border_rings(uint32_t nb, const uint32_t *edges, uint32_t *ring_verts, uint32_t *ring_lens) {
+    std::vector<uint32_t> border(edges, edges + 2 * (size_t)nb);
+    const auto rings = find_border_rings(border);
+    uint32_t k = 0;
+    for (size_t r = 0; r < rings.size(); ++r) {
+        ring_lens[r] = (uint32_t)rings[r].size();
+        for (uint32_t v : rings[r]) ring_verts[k++] = v;
+    }
+    return (uint32_t)rings.size();
+}
+
 // counts: vertices, triangles, error, isle vertices, isle triangles, border
 // edges, holes, hole vertices, hole triangles, skipped rings
 void tsro_mesh_counts(const tsro_mesh *h, uint64_t *c) {

@@ -54,6 +54,8 @@ def lib():
         L.tsro_mesh_free.argtypes = [P]
         L.tsro_mesh_counts.argtypes = [P, P]
         L.tsro_mesh_get.argtypes = [P, P, P, P, P]
+        L.tsro_border_rings.restype = ctypes.c_uint32
+        L.tsro_border_rings.argtypes = [ctypes.c_uint32, P, P, P]
         _lib = L
     return _lib
 
@@ -197,3 +199,18 @@ def mesh_postprocess(positions, triangles, scales=None, min_isle_size=1000):
     finally:
         L.tsro_mesh_free(h)
     return counts, p, n, s, t
+
+
+def border_rings(edges):
+    """FlexibleMesh::findBorderRings on (tail, head) edges in list order;
+    returns the rings as lists of tail vertices."""
+    e = np.ascontiguousarray(edges, np.uint32).reshape(-1, 2)
+    nb = e.shape[0]
+    verts = np.zeros(max(nb, 1), np.uint32)
+    lens = np.zeros(max(nb, 1), np.uint32)
+    n = lib().tsro_border_rings(nb, _p(e), _p(verts), _p(lens))
+    out, k = [], 0
+    for r in range(n):
+        out.append([int(x) for x in verts[k:k + lens[r]]])
+        k += int(lens[r])
+    return out
