@@ -253,8 +253,10 @@ typedef struct {
  * FlexibleMesh.cpp:1227-1259).  counts may be NULL. */
 TSR_API tsr_status tsr_mesh_postprocess(tsr_mesh *mesh, uint32_t min_isle_size, tsr_mesh_post_counts *counts);
 
-/* Vertex normals after tsr_mesh_postprocess, 3 doubles per vertex, HOST
- * memory (zeros when post-processing left no triangles). */
+/* Vertex normals after tsr_mesh_postprocess or of a depth-map mesh, 3
+ * doubles per vertex, HOST memory (zeros when post-processing left no
+ * triangles).  Post-processing drops a depth-map mesh's colours and pixel
+ * map. */
 TSR_API tsr_status tsr_mesh_copy_normals(const tsr_mesh *mesh, double *normals);
 
 /* A mesh from HOST arrays, for tsr_mesh_postprocess of a surface that did
@@ -265,6 +267,32 @@ TSR_API tsr_status tsr_mesh_copy_normals(const tsr_mesh *mesh, double *normals);
 TSR_API tsr_status tsr_mesh_create(const double *positions, const double *scales, uint64_t vertex_count,
                                    const uint32_t *triangles, uint64_t triangle_count, void *cuda_stream,
                                    tsr_mesh **out_mesh);
+
+/* ---- samples from depth maps ---- */
+/* DepthImage::triangulate (Image/DepthImage.cpp:186-461): the depth map
+ * (width x height doubles, HOST, row major, depth along the pixel ray, <= 0
+ * invalid) is triangulated block by block with the reference's depth
+ * discontinuity test, vertices are numbered in the reference's order and
+ * placed at center + normalize((x, y, 1) * hps_to_ray_ws) * depth, coloured
+ * from colors (3 doubles per pixel, HOST) or 0.5 grey, given angle-weighted
+ * normals and, as scale, the mean distance to their neighbours
+ * (FlexibleMesh::findVertexNeighbors order, Mesh::computeVertexScales).
+ * The two row-major 3x3 matrices are the ones the reference computes from
+ * its PinholeCamera: hps_to_ray_vs = inverse viewport x inverse projection,
+ * hps_to_ray_ws = hps_to_ray_vs x inverse rotation (DepthImage.cpp:189-194);
+ * (x, y, 1) * M is a row vector times M.  The mesh's vertices are the
+ * samples Samples::addSamplesViaMesh makes (Samples.cpp:262-272): read them
+ * with tsr_mesh_copy, tsr_mesh_copy_normals and tsr_mesh_copy_colors. */
+TSR_API tsr_status tsr_depth_triangulate(const double *depths, uint32_t width, uint32_t height,
+                                         const double hps_to_ray_vs[9], const double hps_to_ray_ws[9],
+                                         const double center[3], const double *colors, void *cuda_stream,
+                                         tsr_mesh **out_mesh);
+/* Vertex colours of a depth-map mesh, 3 doubles per vertex, HOST. */
+TSR_API tsr_status tsr_mesh_copy_colors(const tsr_mesh *mesh, double *colors);
+/* The vertex of every pixel of a depth-map mesh (width x height, 0xFFFFFFFF
+ * for none), HOST; Scene::loadCameraIndices maps per-pixel views with it
+ * (Scene.cpp:527-573). */
+TSR_API tsr_status tsr_mesh_copy_pixel_map(const tsr_mesh *mesh, uint32_t *pixel_to_vertex);
 
 /* ---- learned pruner (no counterpart in the reference) ---- */
 /* The pruner's per-leaf features of a field, leaves x TSR_MLP_FEATURES floats

@@ -2,8 +2,10 @@
 // the mesh post-processing DualMarchingCells runs after extracting a mesh
 // (DualMarchingCells.cpp:26-39): FlexibleMesh::deleteIsolatedGeometry with
 // IslesEraser, FlexibleMesh::fillHoles and
-// Mesh::computeNormalsWeightedByAngles.  It is the parity checker of the GPU
-// post-processing and nothing else; only tests/ load it.
+// Mesh::computeNormalsWeightedByAngles; and of the depth-map triangulation
+// that creates samples (DepthImage::triangulate, DepthImage.cpp:186-461).
+// It is the parity checker of the GPU versions and nothing else; only tests/
+// load it.
 //
 // Paths below are relative to SurfaceReconstruction/SurfaceReconstruction/
 // of the reference.  The reference's Vector3 (BaseProject, absent from the
@@ -374,12 +376,93 @@ void normals(Mesh &m) {
     for (V3 &n : m.nrm) normalize(n);
 }
 
+// ---- DepthImage::triangulate (DepthImage.cpp:186-461)
+// Vector3 * Matrix3x3 is taken as a row vector times the matrix,
+// out_j = (x m0j + y m1j) + z m2j; Math::SQRT_TWO as sqrt(2) rounded to double.
+constexpr double SQRT_TWO = 1.4142135623730951;
+constexpr double DEPTH_DIFFERENCE_FACTOR = 5.0;   // DepthImage.cpp:25
+
+V3 row_times(V3 v, const double *M) {
+    return {v.x * M[0] + v.y * M[3] + v.z * M[6], v.x * M[1] + v.y * M[4] + v.z * M[7],
+            v.x * M[2] + v.y * M[5] + v.z * M[8]};
+}
+
+inline double length(V3 a) { return std::sqrt(dot(a, a)); }
+
+// DepthImage::isDepthDiscontinuity (DepthImage.cpp:385-400)
+bool discontinuity(const double fp[4], const double d[4], uint32_t v0, uint32_t v1) {
+    const uint32_t closer = d[v0] < d[v1] ? v0 : v1, further = d[v0] < d[v1] ? v1 : v0;
+    double f = DEPTH_DIFFERENCE_FACTOR;
+    if (v0 + v1 == 3) f *= SQRT_TWO;
+    return d[further] - d[closer] > fp[closer] * f;
+}
+
+// DepthImage::triangulateBlock (DepthImage.cpp:218-383)
+uint32_t triangulate_block(std::vector<uint32_t> &indices, std::vector<uint32_t> &pix2v, uint32_t nv, uint32_t x,
+                           uint32_t y, const double *depths, uint32_t W, const double *Mvs) {
+    static const uint32_t tri_of[4][3] = {{0, 2, 1}, {0, 3, 1}, {0, 2, 3}, {1, 2, 3}};
+    const uint32_t p = W * y + x;
+    const double d[4] = {depths[p], depths[p + 1], depths[p + W], depths[p + W + 1]};
+    uint32_t mask = 0, avail = 0;
+    for (uint32_t i = 0; i < 4; ++i) {
+        if (0.0 >= d[i]) continue;
+        mask |= 1u << i;
+        ++avail;
+    }
+    if (avail < 3) return nv;
+    uint32_t t[2] = {INVALID, INVALID};
+    switch (mask) {
+        case 7: t[0] = 0; break;
+        case 11: t[0] = 1; break;
+        case 13: t[0] = 2; break;
+        case 14: t[0] = 3; break;
+        case 15:
+            if (std::fabs(d[0] - d[3]) < std::fabs(d[1] - d[2])) { t[0] = 1; t[1] = 2; }
+            else { t[0] = 0; t[1] = 3; }
+            break;
+        default: return nv;
+    }
+    double fp[4] = {0, 0, 0, 0};
+    for (uint32_t i = 0; i < 4; ++i) {
+        if (0.0 >= d[i]) continue;
+        const V3 v = row_times(V3{(double)(x + i % 2), (double)(y + i / 2), 1.0}, Mvs);
+        fp[i] = Mvs[0] * d[i] / length(v);
+    }
+    for (auto &ti : t) {
+        if (ti == INVALID) continue;
+        for (uint32_t e = 0; e < 3 && ti != INVALID; ++e)
+            if (discontinuity(fp, d, tri_of[ti][e], tri_of[ti][(e + 1) % 3])) ti = INVALID;
+    }
+    for (uint32_t ti : t) {
+        if (ti == INVALID) continue;
+        for (uint32_t c = 0; c < 3; ++c) {
+            const uint32_t q = p + (tri_of[ti][c] / 2) * W + tri_of[ti][c] % 2;
+            if (pix2v[q] == INVALID) pix2v[q] = nv++;
+            indices.push_back(pix2v[q]);
+        }
+    }
+    return nv;
+}
+
+// Mesh::computeAverageDistance (Mesh.cpp:100-123)
+double average_distance(V3 c, const std::vector<V3> &pos, const std::vector<uint32_t> &nbs, uint32_t skip) {
+    uint32_t count = (uint32_t)nbs.size();
+    double sum = 0.0;
+    for (uint32_t n : nbs) {
+        if (n == skip) { --count; continue; }
+        sum += length(pos[n] - c);
+    }
+    if (count == 0) return -1.7976931348623157e308;
+    return sum / count;
+}
+
 }  // namespace
 
 extern "C" {
 
 struct tsro_mesh {
     Mesh m;
+    std::vector<V3> colors;   // depth meshes only
 };
 
 // DualMarchingCells::DualMarchingCells after extractMesh (DualMarchingCells.cpp:
@@ -407,6 +490,63 @@ tsro_mesh *tsro_mesh_postprocess(uint32_t nv, const double *positions, const dou
 }
 
 void tsro_mesh_free(tsro_mesh *h) { delete h; }
+
+// DepthImage::triangulate + createFlexibleMesh (DepthImage.cpp:186-216,
+// 402-461): triangles of the pixel grid, vertex positions along the pixel
+// rays, colours (given per pixel, or 0.5 grey), angle-weighted normals and
+// each vertex's mean distance to its neighbours (FlexibleMesh::
+// findVertexNeighbors, FlexibleMesh.cpp:137-171; Mesh::computeVertexScales,
+// Mesh.cpp:63-98).  pix2v (W*H) receives the vertex of every pixel.
+tsro_mesh *tsro_depth_triangulate(const double *depths, uint32_t W, uint32_t H, const double *Mvs, const double *Mws,
+                                  const double *center, const double *colors, uint32_t *pix2v_out) {
+    auto *h = new tsro_mesh();
+    Mesh &m = h->m;
+    std::vector<uint32_t> pix2v((size_t)W * H, INVALID);
+    uint32_t nv = 0;
+    for (uint32_t y = 0; y + 1 < H; ++y)
+        for (uint32_t x = 0; x + 1 < W; ++x) nv = triangulate_block(m.tri, pix2v, nv, x, y, depths, W, Mvs);
+    // findVertexNeighbors
+    std::vector<std::vector<uint32_t>> nbs(nv);
+    auto add = [&](uint32_t a, uint32_t b) {
+        for (uint32_t q : nbs[a]) if (q == b) return;
+        nbs[a].push_back(b);
+    };
+    for (size_t t = 0; t + 2 < m.tri.size(); t += 3) {
+        uint32_t e0 = m.tri[t], e1 = m.tri[t + 1];
+        for (uint32_t k = 0; k < 3; ++k) {
+            add(e0, e1);
+            add(e1, e0);
+            e0 = e1;
+            e1 = m.tri[t + (k + 2) % 3];
+        }
+    }
+    // setVertexPositions / setVertexColors
+    m.pos.resize(nv);
+    m.nrm.resize(nv);
+    m.scale.assign(nv, 0.0);
+    h->colors.assign(nv, V3{0.5, 0.5, 0.5});
+    const V3 c{center[0], center[1], center[2]};
+    for (uint32_t p = 0; p < W * H; ++p) {
+        const uint32_t v = pix2v[p];
+        if (v == INVALID) continue;
+        V3 dir = row_times(V3{(double)(p % W), (double)(p / W), 1.0}, Mws);
+        normalize(dir);
+        m.pos[v] = c + dir * depths[p];
+        if (colors) h->colors[v] = V3{colors[3 * (size_t)p], colors[3 * (size_t)p + 1], colors[3 * (size_t)p + 2]};
+    }
+    normals(m);
+    for (uint32_t v = 0; v < nv; ++v) m.scale[v] = average_distance(m.pos[v], m.pos, nbs[v], v);
+    if (pix2v_out) std::memcpy(pix2v_out, pix2v.data(), pix2v.size() * sizeof(uint32_t));
+    return h;
+}
+
+void tsro_mesh_colors(const tsro_mesh *h, double *colors) {
+    for (size_t v = 0; v < h->colors.size(); ++v) {
+        colors[3 * v] = h->colors[v].x;
+        colors[3 * v + 1] = h->colors[v].y;
+        colors[3 * v + 2] = h->colors[v].z;
+    }
+}
 
 // The ring search alone: nb border edges (tail, head pairs in list order)
 // into rings of tail vertices; returns the ring count.  ring_verts holds nb

@@ -54,6 +54,9 @@ def lib():
         L.tsro_mesh_free.argtypes = [P]
         L.tsro_mesh_counts.argtypes = [P, P]
         L.tsro_mesh_get.argtypes = [P, P, P, P, P]
+        L.tsro_depth_triangulate.restype = P
+        L.tsro_depth_triangulate.argtypes = [P, ctypes.c_uint32, ctypes.c_uint32, P, P, P, P, P]
+        L.tsro_mesh_colors.argtypes = [P, P]
         L.tsro_border_rings.restype = ctypes.c_uint32
         L.tsro_border_rings.argtypes = [ctypes.c_uint32, P, P, P]
         _lib = L
@@ -214,3 +217,31 @@ def border_rings(edges):
         out.append([int(x) for x in verts[k:k + lens[r]]])
         k += int(lens[r])
     return out
+
+
+def depth_triangulate(depths, hps_to_ray_vs, hps_to_ray_ws, center, colors=None):
+    """DepthImage::triangulate on the CPU: a depth map (H x W, along the
+    rays), the two 3x3 matrices (row vector times matrix) and the centre of
+    projection.  Returns dict positions, normals, scales, colors, triangles,
+    pixel_to_vertex (H x W)."""
+    L = lib()
+    d = np.ascontiguousarray(depths, np.float64)
+    H, W = d.shape
+    mvs = np.ascontiguousarray(hps_to_ray_vs, np.float64).reshape(9)
+    mws = np.ascontiguousarray(hps_to_ray_ws, np.float64).reshape(9)
+    c = np.ascontiguousarray(center, np.float64).reshape(3)
+    col = None if colors is None else np.ascontiguousarray(colors, np.float64).reshape(H * W * 3)
+    pix = np.zeros((H, W), np.uint32)
+    h = L.tsro_depth_triangulate(_p(d), W, H, _p(mvs), _p(mws), _p(c), _p(col), _p(pix))
+    try:
+        cnt = np.zeros(len(MESH_COUNT_KEYS), np.uint64)
+        L.tsro_mesh_counts(h, _p(cnt))
+        nv, nt = int(cnt[0]), int(cnt[1])
+        p, n, s = np.zeros((nv, 3)), np.zeros((nv, 3)), np.zeros(nv)
+        t = np.zeros((nt, 3), np.uint32)
+        L.tsro_mesh_get(h, _p(p), _p(n), _p(s), _p(t))
+        cols = np.zeros((nv, 3))
+        L.tsro_mesh_colors(h, _p(cols))
+    finally:
+        L.tsro_mesh_free(h)
+    return dict(positions=p, normals=n, scales=s, colors=cols, triangles=t, pixel_to_vertex=pix)

@@ -18,7 +18,7 @@ CSRC = PKG / "csrc"
 LIBDIR = PKG / "lib"
 OBJDIR = PKG / "lib" / "obj"
 LIB = LIBDIR / "libtsrcore.so"
-SOURCES = ["capi.cu", "tree.cu", "occupancy.cu", "dmc.cu", "mlp.cu", "noalloc.cu", "files.cu", "meshpost.cu"]
+SOURCES = ["capi.cu", "tree.cu", "occupancy.cu", "dmc.cu", "mlp.cu", "noalloc.cu", "files.cu", "meshpost.cu", "depth.cu"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--extended-lambda", "-Xcompiler", "-fPIC",

@@ -118,6 +118,9 @@ _sig = {
     "tsr_mesh_postprocess": (ctypes.c_int, [_P, ctypes.c_uint32, _P]),
     "tsr_mesh_copy_normals": (ctypes.c_int, [_P, _P]),
     "tsr_mesh_create": (ctypes.c_int, [_P, _P, ctypes.c_uint64, _P, ctypes.c_uint64, _P, _P]),
+    "tsr_depth_triangulate": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.c_uint32, _P, _P, _P, _P, _P, _P]),
+    "tsr_mesh_copy_colors": (ctypes.c_int, [_P, _P]),
+    "tsr_mesh_copy_pixel_map": (ctypes.c_int, [_P, _P]),
     "tsr_tree_save": (ctypes.c_int, [_P, ctypes.c_char_p]),
     "tsr_tree_save_samples": (ctypes.c_int, [_P, _P, ctypes.c_char_p]),
     "tsr_tree_load": (ctypes.c_int, [ctypes.c_char_p, _P, _P, _P, _P, _P]),
@@ -202,6 +205,33 @@ class Samples:
     def view(self):
         return tsr_samples_view(self.count, self.max_cameras_per_sample, _ptr(self.positions), _ptr(self.normals),
                                 _ptr(self.scales), _ptr(self.confidences), _ptr(self.camera_links))
+
+    @classmethod
+    def fromDepthMeshes(cls, meshes, camera_indices):
+        """Samples::addSamplesViaMeshes (Samples.cpp:224-272): one sample per
+        vertex of every DepthMesh, confidence 1, with the mesh's camera links
+        -- ``camera_indices[i]`` is either the reference camera's index (the
+        reference's fallback without a views image, Scene.cpp:563-570) or a
+        (vertices x k) array of camera indices; K is the largest k and shorter
+        link lists are padded with 0xFFFFFFFF (Cameras::INVALID_ID)."""
+        links = []
+        for m, ci in zip(meshes, camera_indices):
+            nv = m.positions.shape[0]
+            if np.ndim(ci) == 0:
+                links.append(np.full((nv, 1), int(ci), np.uint32))
+            else:
+                a = np.asarray(ci, np.uint32).reshape(nv, -1)
+                links.append(a)
+        k = max([a.shape[1] for a in links] + [1])
+        links = [np.pad(a, ((0, 0), (0, k - a.shape[1])), constant_values=INVALID_INDEX) for a in links]
+        pos = np.concatenate([m.positions for m in meshes]) if meshes else np.zeros((0, 3))
+        nrm = np.concatenate([m.normals for m in meshes]) if meshes else np.zeros((0, 3))
+        sc = np.concatenate([m.scales for m in meshes]) if meshes else np.zeros(0)
+        if (sc <= 0).any():   # Samples::check (Samples.cpp:274-288)
+            raise ValueError("invalid (non-positive) sample scale detected")
+        out = cls(pos, nrm, sc, np.ones(pos.shape[0]), np.concatenate(links) if links else np.zeros((0, k)))
+        out.colors = np.concatenate([m.colors for m in meshes]) if meshes else np.zeros((0, 3))
+        return out
 
     def reorder(self, target_indices):
         """Samples::reorder (Samples.cpp:825-835): element i moves to target[i]."""
@@ -615,6 +645,53 @@ class DualMarchingCells:
 
     def getSurface(self):
         return self.positions, self.triangles
+
+
+class DepthImage:
+    """DepthImage (Image/DepthImage.cpp): a depth map along the pixel rays,
+    height x width, values <= 0 invalid."""
+
+    def __init__(self, depths):
+        self.depths = np.ascontiguousarray(depths, np.float64)
+        if self.depths.ndim != 2:
+            raise ValueError("a depth map is height x width")
+
+    def triangulate(self, hps_to_ray_vs, hps_to_ray_ws, center, colors=None, stream=None):
+        """DepthImage::triangulate (DepthImage.cpp:186-216) on the GPU.  The
+        3x3 matrices are the ones the reference computes from its
+        PinholeCamera (inverse viewport x inverse projection, and that x
+        inverse rotation), applied to (x, y, 1) as a row vector."""
+        return DepthMesh(self, hps_to_ray_vs, hps_to_ray_ws, center, colors, stream)
+
+
+class DepthMesh:
+    """The FlexibleMesh DepthImage::triangulate returns: positions, normals,
+    colours, scales, triangles and the vertex of every pixel."""
+
+    def __init__(self, image: DepthImage, hps_to_ray_vs, hps_to_ray_ws, center, colors=None, stream=None):
+        H, W = image.depths.shape
+        mvs = np.ascontiguousarray(hps_to_ray_vs, np.float64).reshape(9)
+        mws = np.ascontiguousarray(hps_to_ray_ws, np.float64).reshape(9)
+        c = np.ascontiguousarray(center, np.float64).reshape(3)
+        col = None if colors is None else np.ascontiguousarray(colors, np.float64).reshape(H * W * 3)
+        h = _P()
+        _check(lib.tsr_depth_triangulate(_ptr(image.depths), W, H, _ptr(mvs), _ptr(mws), _ptr(c),
+                                         _ptr(col) if col is not None else None, _stream_ptr(stream), ctypes.byref(h)))
+        try:
+            cnt = tsr_mesh_counts()
+            _check(lib.tsr_mesh_get_counts(h, ctypes.byref(cnt)))
+            nv, nt = int(cnt.vertices), int(cnt.triangles)
+            self.positions, self.normals, self.colors = np.zeros((nv, 3)), np.zeros((nv, 3)), np.zeros((nv, 3))
+            self.scales = np.zeros(nv)
+            self.triangles = np.zeros((nt, 3), np.uint32)
+            self.pixel_to_vertex = np.zeros((H, W), np.uint32)
+            _check(lib.tsr_mesh_copy(h, None, _ptr(self.positions), _ptr(self.scales), None, _ptr(self.triangles)))
+            if nv:
+                _check(lib.tsr_mesh_copy_normals(h, _ptr(self.normals)))
+                _check(lib.tsr_mesh_copy_colors(h, _ptr(self.colors)))
+            _check(lib.tsr_mesh_copy_pixel_map(h, _ptr(self.pixel_to_vertex)))
+        finally:
+            lib.tsr_mesh_free(h)
 
 
 class Pruner:

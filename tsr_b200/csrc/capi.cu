@@ -507,7 +507,8 @@ tsr_status tsr_mesh_postprocess(tsr_mesh *m, uint32_t min_isle_size, tsr_mesh_po
 tsr_status tsr_mesh_copy_normals(const tsr_mesh *m, double *normals) {
     return guarded([&] {
         if (!m || !normals) fail(TSR_ERR_INVALID_ARG, "null argument");
-        if (m->vnrm.n != 3 * m->n_verts) fail(TSR_ERR_STATE, "normals exist after tsr_mesh_postprocess only");
+        if (m->vnrm.n != 3 * m->n_verts)
+            fail(TSR_ERR_STATE, "normals exist after tsr_mesh_postprocess and for depth-map meshes only");
         to_host(m->vnrm, 3 * m->n_verts, normals, m->stream);
         TSR_CUDA(cudaStreamSynchronize(m->stream));
     });
@@ -548,6 +549,43 @@ tsr_status tsr_mesh_create(const double *positions, const double *scales, uint64
             throw;
         }
         *out = m;
+    });
+}
+
+tsr_status tsr_depth_triangulate(const double *depths, uint32_t width, uint32_t height, const double *hps_to_ray_vs,
+                                 const double *hps_to_ray_ws, const double *center, const double *colors,
+                                 void *cuda_stream, tsr_mesh **out) {
+    if (out) *out = nullptr;
+    return guarded([&] {
+        if (!depths || !hps_to_ray_vs || !hps_to_ray_ws || !center || !out) fail(TSR_ERR_INVALID_ARG, "null argument");
+        tsr_mesh *m = new tsr_mesh();
+        m->stream = (cudaStream_t)cuda_stream;
+        try {
+            triangulate_depth(depths, width, height, hps_to_ray_vs, hps_to_ray_ws, center, colors, *m);
+        } catch (...) {
+            delete m;
+            throw;
+        }
+        *out = m;
+    });
+}
+
+tsr_status tsr_mesh_copy_colors(const tsr_mesh *m, double *colors) {
+    return guarded([&] {
+        if (!m || !colors) fail(TSR_ERR_INVALID_ARG, "null argument");
+        if (m->vcol.n != 3 * m->n_verts) fail(TSR_ERR_STATE, "colours exist for depth-map meshes only");
+        to_host(m->vcol, 3 * m->n_verts, colors, m->stream);
+        TSR_CUDA(cudaStreamSynchronize(m->stream));
+    });
+}
+
+tsr_status tsr_mesh_copy_pixel_map(const tsr_mesh *m, uint32_t *pixel_to_vertex) {
+    return guarded([&] {
+        if (!m || !pixel_to_vertex) fail(TSR_ERR_INVALID_ARG, "null argument");
+        const size_t np = (size_t)m->width * m->height;
+        if (np == 0 || m->pix2v.n != np) fail(TSR_ERR_STATE, "a pixel map exists for depth-map meshes only");
+        to_host(m->pix2v, np, pixel_to_vertex, m->stream);
+        TSR_CUDA(cudaStreamSynchronize(m->stream));
     });
 }
 

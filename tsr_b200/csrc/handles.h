@@ -58,6 +58,9 @@ struct tsr_mesh {
     tsr::DBuf<double> vpos, vscale;
     tsr::DBuf<uint32_t> vkeys, tris;
     tsr::DBuf<double> vnrm;            // 3 per vertex once post-processed; empty before
+    tsr::DBuf<double> vcol;            // 3 per vertex, depth-map meshes only
+    tsr::DBuf<uint32_t> pix2v;         // vertex of every pixel, depth-map meshes only
+    uint32_t width = 0, height = 0;    // depth-map meshes only
 };
 
 namespace tsr {
@@ -78,6 +81,10 @@ void pruner_predict(const tsr_tree &t, const tsr_pruner &pr, const double *esum,
                     double threshold, DBuf<uint8_t> &pred, cudaStream_t st);
 void extract_dmc(const tsr_tree &t, const tsr_occupancy &o, tsr_mesh &m);
 void postprocess_mesh(tsr_mesh &m, uint32_t min_isle_size, tsr_mesh_post_counts &counts);
+void angle_weighted_normals(const uint32_t *tris, uint32_t nt, const double *pos, uint32_t nv, double *nrm,
+                            cudaStream_t st);
+void triangulate_depth(const double *depths_host, uint32_t width, uint32_t height, const double *hps_to_ray_vs,
+                       const double *hps_to_ray_ws, const double *center, const double *colors_host, tsr_mesh &m);
 void reserve_pool(size_t want, cudaStream_t st);
 void root_scope_noalloc(uint64_t count, const double *positions, const double *scales, double h_svo,
                         double *out_min_xyz_size, cudaStream_t st);

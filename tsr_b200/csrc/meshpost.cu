@@ -388,6 +388,14 @@ int bits_for(uint32_t maxval) {
 
 }  // namespace
 
+// Mesh::computeNormalsWeightedByAngles (Mesh.cpp:145-203) into nrm, which
+// must hold zeros.
+void angle_weighted_normals(const uint32_t *tris, uint32_t nt, const double *pos, uint32_t nv, double *nrm,
+                            cudaStream_t st) {
+    if (nt) k_angle_normals<<<grid_for(nt, BLK), BLK, 0, st>>>(nt, tris, pos, nrm); ::tsr::note_launch();
+    if (nv) k_normalize<<<grid_for(nv, BLK), BLK, 0, st>>>(nv, nrm); ::tsr::note_launch();
+}
+
 void postprocess_mesh(tsr_mesh &m, uint32_t min_isle_size, tsr_mesh_post_counts &pc) {
     cudaStream_t st = m.stream;
     pc = tsr_mesh_post_counts{};
@@ -527,10 +535,7 @@ void postprocess_mesh(tsr_mesh &m, uint32_t min_isle_size, tsr_mesh_post_counts 
     }
     // ---- normals (Mesh.cpp:145-203); zeros when nothing is left
     nrm.zero();
-    if (rest) {
-        k_angle_normals<<<grid_for(nt2, BLK), BLK, 0, st>>>(nt2, tris_p, pos_p, nrm.p); ::tsr::note_launch();
-        k_normalize<<<grid_for(nv2, BLK), BLK, 0, st>>>(nv2, nrm.p); ::tsr::note_launch();
-    }
+    if (rest) angle_weighted_normals(tris_p, nt2, pos_p, nv2, nrm.p, st);
     TSR_CUDA(cudaStreamSynchronize(st));   // every step ran: from here on nothing can fail
     if (grow) {
         m.vpos = std::move(pos2);
@@ -546,6 +551,10 @@ void postprocess_mesh(tsr_mesh &m, uint32_t min_isle_size, tsr_mesh_post_counts 
     m.vnrm = std::move(nrm);
     m.n_verts = nv2;
     m.n_tris = nt2;
+    // a depth-map mesh's colours and pixel map describe the old vertices
+    m.vcol.release();
+    m.pix2v.release();
+    m.width = m.height = 0;
 }
 
 }  // namespace tsr

@@ -326,3 +326,47 @@ def random_csg_scene(seed, n_target=3_000_000, width=800, height=600, f=600.0, n
 def tiny_scene(seed=0, stride=16):
     """A few thousand samples of the sphere scene, for fast tests."""
     return sphere_scene(seed=seed, stride=stride)
+
+
+def depth_views(prims, cams, width, height, f, noise_rel, rng, bound_radius=2.5):
+    """Per camera a depth map along the pixel rays (height x width, -1 where
+    nothing is hit) with the two matrices DepthImage::triangulate takes:
+    (x, y, 1) times ``hps_to_ray_vs`` is the pixel's view-space ray
+    ((x + 0.5 - w/2) / f, (y + 0.5 - h/2) / f, 1); times ``hps_to_ray_ws`` its
+    world-space ray (right, down, forward basis of the camera looking at the
+    origin).  The stand-in for the reference's rendered or captured depth
+    maps (SyntheticScene.cpp:45-336)."""
+    views = []
+    A = np.array([[1.0 / f, 0.0, 0.0], [0.0, 1.0 / f, 0.0],
+                  [(0.5 - 0.5 * width) / f, (0.5 - 0.5 * height) / f, 1.0]])
+    ys, xs = np.mgrid[0:height, 0:width]
+    hps = np.stack([xs.ravel().astype(float), ys.ravel().astype(float), np.ones(xs.size)], 1)
+    for cam in np.asarray(cams, float):
+        right, down, fwd = look_at_basis(cam, np.zeros(3))
+        B = np.stack([right, down, fwd])
+        Mws = A @ B
+        d = hps @ Mws
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        best = np.full(d.shape[0], np.inf)
+        b = d @ cam
+        near = b * b - (cam @ cam - bound_radius * bound_radius) >= 0
+        for pr in prims:
+            t = np.full(d.shape[0], np.inf)
+            if near.any():
+                t[near] = pr.hit(cam, d[near])
+            best = np.minimum(best, t)
+        ok = np.isfinite(best)
+        depth = np.where(ok, best * (1.0 + rng.normal(0.0, noise_rel, best.shape)), -1.0)
+        views.append(dict(depths=depth.reshape(height, width), hps_to_ray_vs=A, hps_to_ray_ws=Mws,
+                          center=cam.copy()))
+    return views
+
+
+def sphere_depth_views(seed=0, width=160, height=120, f=125.0, n_cams=6):
+    """Depth maps of the unit sphere in front of a plate (a depth jump at the
+    silhouette) from cameras on a ring of radius 3."""
+    rng = np.random.default_rng(seed)
+    cams = [[3 * math.cos(2 * math.pi * k / n_cams), 3 * math.sin(2 * math.pi * k / n_cams), 0.4]
+            for k in range(n_cams)]
+    prims = [Sphere([0, 0, 0], 1.0), Box([-2.2, -2.2, -1.6], [2.2, 2.2, -1.5])]
+    return depth_views(prims, cams, width, height, f, 0.001, rng)
