@@ -16,6 +16,10 @@ cone-kernel passes, priors, occupancy values and DMC.
   every step.
 * ``--impl reference`` -- the FP64 CPU oracle (a restatement of the reference's
   C++ path, which cannot be built here) on the host cores, same metric.
+* ``next_rows`` (1 GPU, not timed into the headline) -- the paths either side
+  of the hot path with the CPU restatement timed beside each: the crust's
+  post-processing, depth-map triangulation, the incremental field update
+  and the tree/field files (``--no-next-rows`` skips them).
 
 Multi-GPU: replicas only (each rank reconstructs its own seeded scene; there
 is no data-path collective); value = all ranks' samples / max rank time.
@@ -407,11 +411,173 @@ def our_arm(args):
         line["cpu_baseline"] = {"value": cs.n / tcpu, "unit": UNIT, "cores": threads, "kind": "port",
                                 "sample": "FP64 oracle full pipeline on the same geometry and cameras at %d samples"
                                 % cs.n}
+    if rank == 0 and world == 1 and not args.no_next_rows:
+        line["next_rows"] = next_rows(core, scene, cams, params, stream, line["ms_per_step"],
+                                      cpu=not args.no_cpu_baseline)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def next_rows(core, scene, cams, params, stream, ms_per_step, cpu=True):
+    """Measurements of the paths either side of the hot path, on this GPU with
+    the CPU restatement timed beside each: the crust's post-processing
+    (DualMarchingCells.cpp:31-36), depth-map triangulation (the samples'
+    source, DepthImage::triangulate), the incremental field update
+    (Occupancy::eraseSamples) and the tree/field files.  Each entry is
+    independent and reports an error instead of failing the run."""
+    import ctypes
+    import tempfile
+
+    import numpy as np
+    import torch
+    from oracle import pyoracle
+    from tsr_b200 import scenes
+
+    hbm, src = peaks()
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+    out = {}
+
+    def ev_ms(fn, reps):
+        ms = []
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            prep = fn(None)
+            a.record(stream)
+            fn(prep)
+            b.record(stream)
+            torch.cuda.synchronize()
+            ms.append(a.elapsed_time(b))
+        return ms
+
+    samples = core.Samples(scene.pos, scene.nrm, scene.scale, scene.conf, scene.links)
+    tree = core.Tree(samples, params, stream=stream, reorder_samples=False)
+    occ = core.Occupancy(tree, cams, params, stream=stream)
+    try:
+        raw = occ.extractCrust(stream=stream)
+        holder = {}
+
+        def post(prep):
+            if prep is None:   # a fresh raw mesh, untimed
+                h = ctypes.c_void_p()
+                core._check(core.lib.tsr_dmc_extract(tree.handle, occ.handle, sptr, ctypes.byref(h)))
+                holder["h"] = h
+                return h
+            pc = core.tsr_mesh_post_counts()
+            core._check(core.lib.tsr_mesh_postprocess(prep, 1000, ctypes.byref(pc)))
+            holder["pc"] = pc
+            core.lib.tsr_mesh_free(prep)
+
+        post(post(None))
+        ms = ev_ms(post, 5)
+        pc = holder["pc"]
+        nv, nt = raw.positions.shape[0], raw.triangles.shape[0]
+        oc, tcpu = None, None
+        if cpu:
+            t0 = time.perf_counter()
+            oc = pyoracle.mesh_postprocess(raw.positions, raw.triangles, raw.scales, 1000)[0]
+            tcpu = time.perf_counter() - t0
+        alg = nt * 12 * 2 + nv * 24 * 3     # triangles read twice; positions read twice, normals written
+        gpu_ms = statistics.median(ms)
+        out["mesh_postprocess"] = {
+            "what": "isle deletion (min 1000 vertices), hole filling, angle-weighted normals of this workload's "
+                    "crust", "vertices": nv, "triangles": nt,
+            "isle_vertices": pc.isle_vertices, "holes": pc.holes, "hole_triangles": pc.hole_triangles,
+            "gpu_ms": gpu_ms, "cpu_ms": None if tcpu is None else 1e3 * tcpu,
+            "cpu": "CPU restatement, 1 thread (kind: port)",
+            "same_counts_as_cpu": None if oc is None else bool(
+                oc["triangles"] == nt - pc.isle_triangles + pc.hole_triangles),
+            "roofline": {"bound": "hbm", "algorithmic_bytes": alg, "achieved": alg / gpu_ms / 1e6, "peak": hbm,
+                         "unit": "GB/s", "frac": alg / gpu_ms / 1e6 / hbm, "peak_source": src,
+                         "note": "sorts, scans and one-thread ring search over a small mesh: launch-bound"}}
+    except Exception as e:   # pragma: no cover - reported, not fatal
+        out["mesh_postprocess"] = {"error": repr(e)}
+    try:
+        views = scenes.sphere_depth_views(width=1280, height=960, f=600.0, n_cams=4)
+
+        def tri(prep, v=views[0]):
+            if prep is None:
+                return True
+            core.DepthImage(v["depths"]).triangulate(v["hps_to_ray_vs"], v["hps_to_ray_ws"], v["center"],
+                                                     stream=stream)
+
+        tri(True)
+        ms = ev_ms(tri, 4)
+        v = views[0]
+        g = core.DepthImage(v["depths"]).triangulate(v["hps_to_ray_vs"], v["hps_to_ray_ws"], v["center"],
+                                                     stream=stream)
+        tcpu = None
+        if cpu:
+            t0 = time.perf_counter()
+            pyoracle.depth_triangulate(v["depths"], v["hps_to_ray_vs"], v["hps_to_ray_ws"], v["center"])
+            tcpu = time.perf_counter() - t0
+        npx = v["depths"].size
+        nv, nt = g.positions.shape[0], g.triangles.shape[0]
+        alg = npx * (8 + 4) + nv * (24 * 4 + 8) + nt * 12
+        gpu_ms = statistics.median(ms)
+        out["depth_triangulate"] = {
+            "what": "DepthImage::triangulate of a 1280x960 depth map (sphere and plate), through the C ABI "
+                    "from host memory (H2D of the map, mesh read back)",
+            "pixels": npx, "vertices": nv, "triangles": nt, "gpu_ms": gpu_ms,
+            "cpu_ms": None if tcpu is None else 1e3 * tcpu,
+            "pixels_per_s_gpu": npx / gpu_ms * 1e3, "pixels_per_s_cpu": None if tcpu is None else npx / tcpu,
+            "cpu": "CPU restatement, 1 thread (kind: port)",
+            "roofline": {"bound": "hbm", "algorithmic_bytes": alg, "achieved": alg / gpu_ms / 1e6, "peak": hbm,
+                         "unit": "GB/s", "frac": alg / gpu_ms / 1e6 / hbm, "peak_source": src}}
+    except Exception as e:   # pragma: no cover
+        out["depth_triangulate"] = {"error": repr(e)}
+    try:
+        rng = np.random.default_rng(7)
+        chosen = np.sort(rng.choice(tree.sample_count, size=tree.sample_count // 100, replace=False))
+
+        def upd(prep):
+            if prep is None:
+                holder["o"] = core.Occupancy(tree, cams, params, stream=stream)
+                return True
+            holder["o"].eraseSamples(chosen, cams, params)
+
+        upd(upd(None))
+        ms = ev_ms(upd, 3)
+        out["occupancy_update"] = {
+            "what": "Occupancy::eraseSamples of 1% of the samples (both cone passes over their links with "
+                    "negated values, then priors and values of every leaf)",
+            "samples_removed": int(chosen.shape[0]), "gpu_ms": statistics.median(ms),
+            "full_step_ms": ms_per_step}
+    except Exception as e:   # pragma: no cover
+        out["occupancy_update"] = {"error": repr(e)}
+    try:
+        with tempfile.TemporaryDirectory() as d:
+            prefix = os.path.join(d, "scene.octree")
+            t0 = time.perf_counter()
+            tree.saveToFiles(prefix)
+            occ.saveToFile(os.path.join(d, "scene.occupancy"))
+            tsave = time.perf_counter() - t0
+            nbytes = sum(os.path.getsize(os.path.join(d, f)) for f in os.listdir(d))
+            ordered = core.Samples(*_tree_samples(core, tree, scene.k))
+            t0 = time.perf_counter()
+            t2 = core.Tree.fromFiles(prefix, ordered, params=params, stream=stream)
+            core.Occupancy.fromFile(t2, os.path.join(d, "scene.occupancy"), params, stream=stream)
+            tload = time.perf_counter() - t0
+        out["files"] = {"what": "tree (.nodes/.leaves/.dualCells) and field (.occupancy) of this workload: "
+                                "save, then load with full validation (host I/O and checks)",
+                        "bytes": nbytes, "save_s": tsave, "load_s": tload,
+                        "save_gb_s": nbytes / tsave / 1e9, "load_gb_s": nbytes / tload / 1e9}
+    except Exception as e:   # pragma: no cover
+        out["files"] = {"error": repr(e)}
+    return out
+
+
+def _tree_samples(core, tree, k):
+    """The tree's samples in tree order (what a .samples file holds)."""
+    import numpy as np
+    n = tree.sample_count
+    pos, nrm, sc, cf = np.zeros((n, 3)), np.zeros((n, 3)), np.zeros(n), np.zeros(n)
+    links = np.zeros((n, k), np.uint32)
+    core._check(core.lib.tsr_tree_copy_samples(tree.handle, core._ptr(pos), core._ptr(nrm), core._ptr(sc),
+                                               core._ptr(cf), core._ptr(links)))
+    return pos, nrm, sc, cf, links
 
 
 def main():
@@ -424,6 +590,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--value-only", action="store_true", help="skip the e2e leg (profiling runs)")
     ap.add_argument("--no-pruned", action="store_true", help="skip the learned pruner's leg")
+    ap.add_argument("--no-next-rows", action="store_true",
+                    help="skip the measurements of post-processing, depth maps, updates and files")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)
