@@ -223,3 +223,54 @@ def test_samples_file_round_trip(name, tmp_path):
         np.testing.assert_array_equal(d[k], v)
     k = s.camera_links.shape[1]
     assert (tmp_path / "s.samples").stat().st_size == 16 + 8 + 48 + s.count * (72 + 16 + 4 * k)
+
+
+def test_mesh_and_depth_arguments_rejected_on_the_host():
+    """tsr_mesh_create and tsr_depth_triangulate check their arguments before
+    any device work."""
+    import ctypes
+    from tsr_b200 import core
+    h = ctypes.c_void_p()
+    pos = np.zeros((3, 3))
+    bad = np.array([[0, 1, 3]], np.uint32)
+    rc = core.lib.tsr_mesh_create(core._ptr(pos), None, 3, core._ptr(bad), 1, None, ctypes.byref(h))
+    assert core.STATUS[rc] == "TSR_ERR_INVALID_ARG" and "out of range" in core.lib.tsr_last_error_message().decode()
+    assert not h.value
+    rc = core.lib.tsr_mesh_create(None, None, 3, None, 0, None, ctypes.byref(h))
+    assert core.STATUS[rc] == "TSR_ERR_INVALID_ARG"
+    m = np.eye(3)
+    c = np.zeros(3)
+    d = np.ones((1, 5))
+    rc = core.lib.tsr_depth_triangulate(core._ptr(d), 5, 1, core._ptr(m), core._ptr(m), core._ptr(c), None, None,
+                                        ctypes.byref(h))
+    assert core.STATUS[rc] == "TSR_ERR_INVALID_ARG" and "2 x 2" in core.lib.tsr_last_error_message().decode()
+    rc = core.lib.tsr_depth_triangulate(None, 5, 5, core._ptr(m), core._ptr(m), core._ptr(c), None, None,
+                                        ctypes.byref(h))
+    assert core.STATUS[rc] == "TSR_ERR_INVALID_ARG"
+    assert core.STATUS[core.lib.tsr_mesh_postprocess(None, 1, None)] == "TSR_ERR_INVALID_ARG"
+
+
+class _FakeDepthMesh:
+    def __init__(self, n, seed):
+        rng = np.random.default_rng(seed)
+        self.positions = rng.random((n, 3))
+        self.normals = rng.random((n, 3))
+        self.scales = rng.random(n) + 0.1
+        self.colors = rng.random((n, 3))
+
+
+def test_samples_from_depth_meshes():
+    """Samples::addSamplesViaMeshes: concatenation, confidence 1, links of
+    the reference camera or per-vertex lists padded to the largest K."""
+    from tsr_b200 import core
+    a, b = _FakeDepthMesh(4, 0), _FakeDepthMesh(3, 1)
+    s = core.Samples.fromDepthMeshes([a, b], [7, np.array([[1, 2], [3, 4], [5, 6]])])
+    assert s.count == 7 and s.max_cameras_per_sample == 2
+    np.testing.assert_array_equal(s.positions, np.vstack([a.positions, b.positions]))
+    np.testing.assert_array_equal(s.colors, np.vstack([a.colors, b.colors]))
+    np.testing.assert_array_equal(s.confidences, 1.0)
+    np.testing.assert_array_equal(s.camera_links[:4], [[7, 0xFFFFFFFF]] * 4)
+    np.testing.assert_array_equal(s.camera_links[4:], [[1, 2], [3, 4], [5, 6]])
+    a.scales[2] = 0.0
+    with pytest.raises(ValueError, match="non-positive"):
+        core.Samples.fromDepthMeshes([a], [0])
