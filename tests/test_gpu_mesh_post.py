@@ -5,14 +5,16 @@ filled: the fill uses the reference's FP64 expression order with correctly
 rounded operations on both sides) and every scale.  Tolerance: the vertex
 normals, NORMAL_ATOL -- the GPU sums the angle-weighted triangle normals
 with atomics in no fixed order and CUDA's acos may differ from the host's
-in the last bits.
+in the last bits -- except at the rare vertices whose weighted normals
+cancel (sum below ILL_CONDITIONED_SUM), whose direction no summation order
+fixes (check_normals).
 """
 import numpy as np
 import pytest
 
 from oracle import pyoracle
 
-from test_mesh_oracle import uv_sphere
+from test_mesh_oracle import check_normals, uv_sphere
 
 pytestmark = pytest.mark.gpu
 
@@ -31,7 +33,7 @@ def _compare(mesh, positions, triangles, scales, min_isle):
     np.testing.assert_array_equal(mesh.triangles, t)
     np.testing.assert_array_equal(mesh.positions, p)
     np.testing.assert_array_equal(mesh.scales, s)
-    np.testing.assert_allclose(mesh.normals, n, rtol=0, atol=NORMAL_ATOL)
+    check_normals(mesh.normals, n, p, t, NORMAL_ATOL)
     return c
 
 
