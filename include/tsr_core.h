@@ -18,7 +18,16 @@
  *                          priors, cone count   Occupancy.cpp:570-597, Occupancy.h:72-86,192-210
  *   tsr_dmc_extract        DualMarchingCells::DualMarchingCells -> extractMesh
  *                          SurfaceExtraction/DualMarchingCells.cpp:26-169
- *                          (the FlexibleMesh post-processing at :31-36 stays with the caller)
+ *   tsr_mesh_postprocess   its FlexibleMesh post-processing (:31-36): deleteIsolatedGeometry,
+ *                          fillHoles, computeNormalsWeightedByAngles (Geometry/FlexibleMesh.cpp,
+ *                          Geometry/IslesEraser.cpp, Geometry/Mesh.cpp:145-203)
+ *   tsr_occupancy_update   Occupancy::addSamples / eraseSamples (Occupancy.h:167-175)
+ *   tsr_tree_erase_samples Tree::eraseSamples (Tree.cpp:50-53) + Samples::compact
+ *   tsr_tree_save/_load, tsr_tree_save_samples, tsr_occupancy_save/_load
+ *                          Tree::saveToFiles / Tree(filesBeginning), Samples::saveToFile,
+ *                          Occupancy::saveToFile / Occupancy(fileName)
+ *   tsr_depth_triangulate  DepthImage::triangulate (Image/DepthImage.cpp:186-461), the samples'
+ *                          source in Scene::loadDepthMeshes (Scene.cpp:484-525)
  *   tsr_*_free             the owning deletes in Scene (Scene.cpp:627-670)
  *
  * Errors: every call returns a tsr_status; the reference throws

@@ -118,6 +118,7 @@ void upload(DBuf<T> &b, const std::vector<T> &h, cudaStream_t st) {
 }  // namespace
 
 void save_tree(const tsr_tree &t, const std::string &prefix) {
+    if (t.n_nb >= INVALID) fail(TSR_ERR_OVERFLOW_U32, "neighbour count beyond the format's 32-bit count");
     cudaStream_t st = t.stream;
     const uint32_t nn = t.n_nodes, nl = t.n_leaves;
     auto children = download(t.children, nn, st), parents = download(t.parents, nn, st);
