@@ -367,6 +367,13 @@ def our_arm(args):
                      "share_of_step": stages[dom] / total_ms if total_ms else None, "traffic": traffic,
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per unit on csg1m, "
                                        "scaled to this run's units"},
+        # the survey's secondary figures: the traversals' work rates (what bounds them, not HBM)
+        "secondary": {
+            "node_tests_per_s": {"sampleness": oc.visited_sampleness / (stages["occ.sampleness"] / 1e3),
+                                 "emptiness": oc.visited_emptiness / (stages["occ.emptiness"] / 1e3),
+                                 "priors": oc.visited_priors / (stages["occ.priors"] / 1e3)},
+            "accepted_pairs_per_s": {"sampleness": oc.accepted_sampleness / (stages["occ.sampleness"] / 1e3),
+                                     "emptiness": oc.accepted_emptiness / (stages["occ.emptiness"] / 1e3)}},
         "clocks": clk,
     }
     # ---- the learned pruner's field (same workload, same timing), judged by
