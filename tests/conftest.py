@@ -1,5 +1,4 @@
 """Shared fixtures: seeded scenes, the oracle and the GPU library."""
-import os
 import sys
 from pathlib import Path
 

@@ -122,7 +122,6 @@ def test_tree_erase_samples_compacts(built):
     np.testing.assert_array_equal(nodes.sample_start_indices, starts0 - erased_before[starts0])
     # the compacted samples are the kept ones, in order
     pos = np.zeros((kept, 3))
-    import ctypes
     core._check(core.lib.tsr_tree_copy_samples(tree.handle, core._ptr(pos), None, None, None, None))
     np.testing.assert_array_equal(pos, s.positions[inl])
     perm = tree.getPermutation()

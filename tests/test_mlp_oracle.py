@@ -2,7 +2,6 @@
 the oracle's analytic gradient against central differences, the parameter
 layout shared with the C ABI, and the label/threshold helpers."""
 import numpy as np
-import pytest
 
 from oracle import mlp_oracle as mo
 
