@@ -87,3 +87,18 @@ def test_samples_from_depth_maps_reconstruct_the_sphere():
     near_sphere = np.abs(np.linalg.norm(p, axis=1) - 1.0) < 0.05
     near_plate = np.abs(p[:, 2] + 1.5) < 0.1
     assert (near_sphere | near_plate).mean() > 0.8
+
+
+def test_golden_depth_view():
+    """The committed fixture: a 96x72 view with per-pixel colours."""
+    from pathlib import Path
+    from tsr_b200 import core
+    g = np.load(Path(__file__).resolve().parent / "golden" / "depth_small.npz")
+    m = core.DepthImage(g["depth_in"]).triangulate(g["depth_in_mvs"], g["depth_in_mws"], g["depth_in_center"],
+                                                   colors=g["depth_in_colors"])
+    np.testing.assert_array_equal(m.triangles, g["depth_triangles"])
+    np.testing.assert_array_equal(m.pixel_to_vertex, g["depth_pixel_to_vertex"])
+    np.testing.assert_array_equal(m.positions, g["depth_positions"])
+    np.testing.assert_array_equal(m.colors, g["depth_colors"])
+    np.testing.assert_array_equal(m.scales, g["depth_scales"])
+    check_normals(m.normals, g["depth_normals"], g["depth_positions"], g["depth_triangles"], NORMAL_ATOL)

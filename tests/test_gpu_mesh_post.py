@@ -116,3 +116,20 @@ def test_create_rejects_bad_indices():
     from tsr_b200 import core
     with pytest.raises(core.TsrError, match="out of range"):
         core.DualMarchingCells.fromArrays(np.zeros((3, 3)), np.array([[0, 1, 3]], np.uint32))
+
+
+def test_golden_damaged_mesh():
+    """The committed fixture (the sphere fixture's DMC mesh with 3 % of its
+    triangles removed: about a thousand holes, isles below 50 vertices)."""
+    from pathlib import Path
+    from tsr_b200 import core
+    g = np.load(Path(__file__).resolve().parent / "golden" / "mesh_post.npz")
+    mesh = core.DualMarchingCells.fromArrays(g["post_in_pos"], g["post_in_tris"], scales=g["post_in_scale"],
+                                             min_isle_size=int(g["post_min_isle"]))
+    for k in ("isle_vertices", "isle_triangles", "border_edges", "holes", "hole_vertices", "hole_triangles",
+              "skipped_rings"):
+        assert mesh.post_counts[k] == int(g["post_" + k]), k
+    np.testing.assert_array_equal(mesh.triangles, g["post_tris"])
+    np.testing.assert_array_equal(mesh.positions, g["post_pos"])
+    np.testing.assert_array_equal(mesh.scales, g["post_scale"])
+    check_normals(mesh.normals, g["post_nrm"], g["post_pos"], g["post_tris"], NORMAL_ATOL)

@@ -183,3 +183,34 @@ def test_mesh_well_formed(tiny_scene):
     assert np.all((occ == -1e-6) | (occ > 0) | np.isnan(occ))
     pr = f["prior"][np.isfinite(f["prior"])]
     assert pr.min() >= 0 and pr.max() <= 1
+
+
+def test_mesh_post_golden():
+    """The post-processing restatement on the committed damaged mesh (holes,
+    isles) reproduces its committed outputs."""
+    sys.path.insert(0, str(GOLDEN))
+    from make_golden import mesh_post_outputs
+    g = dict(np.load(GOLDEN / "mesh_post.npz"))
+    out = mesh_post_outputs(g)
+    for k, v in out.items():
+        if k == "post_nrm":
+            np.testing.assert_allclose(v, g[k], rtol=0, atol=1e-12, err_msg=k)
+        else:
+            np.testing.assert_array_equal(v, g[k], err_msg=k)
+    assert int(g["post_holes"]) > 100 and int(g["post_isle_vertices"]) > 0
+
+
+def test_depth_golden():
+    """The depth-map triangulation restatement reproduces its committed outputs."""
+    sys.path.insert(0, str(GOLDEN))
+    from make_golden import depth_inputs, depth_outputs
+    g = dict(np.load(GOLDEN / "depth_small.npz"))
+    fresh = depth_inputs()
+    for k, v in fresh.items():
+        np.testing.assert_array_equal(v, g[k], err_msg=k)
+    out = depth_outputs(g)
+    for k, v in out.items():
+        if k == "depth_normals":
+            np.testing.assert_allclose(v, g[k], rtol=0, atol=1e-12, err_msg=k)
+        else:
+            np.testing.assert_array_equal(v, g[k], err_msg=k)
