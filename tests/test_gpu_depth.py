@@ -4,8 +4,9 @@ restatement, and samples made from depth maps through the whole pipeline.
 Bit-exact: triangles, the pixel-to-vertex map, vertex positions, colours and
 scales (the neighbour distances are summed in findVertexNeighbors order with
 correctly rounded operations on both sides).  Tolerance: normals,
-NORMAL_ATOL (FP64 atomic sums in no fixed order, CUDA's acos), except at
-vertices whose weighted normals cancel (check_normals).
+NORMAL_ATOL (FP64 atomic sums in no fixed order, CUDA's acos), widened by
+the sum's condition number where the weighted normals nearly cancel
+(check_normals).
 """
 import numpy as np
 import pytest

@@ -5,9 +5,11 @@ filled: the fill uses the reference's FP64 expression order with correctly
 rounded operations on both sides) and every scale.  Tolerance: the vertex
 normals, NORMAL_ATOL -- the GPU sums the angle-weighted triangle normals
 with atomics in no fixed order and CUDA's acos may differ from the host's
-in the last bits -- except at the rare vertices whose weighted normals
-cancel (sum below ILL_CONDITIONED_SUM), whose direction no summation order
-fixes (check_normals).
+in the last bits -- widened by the sum's condition number where the
+weighted normals nearly cancel (check_normals): there the summation order
+decides the direction, for the reference's OpenMP atomics as for the GPU.
+The CPU restatement itself, fed the same triangles in another order,
+differs at 10-17 such vertices of the golden damaged mesh.
 """
 import numpy as np
 import pytest

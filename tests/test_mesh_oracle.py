@@ -46,14 +46,19 @@ def edge_uses(T):
     return c
 
 
-def normal_sum_magnitude(positions, triangles):
-    """|sum of angle-weighted unit triangle normals| per vertex, in numpy (the
-    quantity Mesh::computeNormalsWeightedByAngles normalises)."""
+def normal_sums(positions, triangles, order=None):
+    """Per vertex: the sum of angle-weighted unit triangle normals (what
+    Mesh::computeNormalsWeightedByAngles normalises) and the sum of the
+    weights (the corner angles), in numpy; ``order`` permutes the triangles'
+    accumulation."""
     p = np.asarray(positions, np.float64)
     t = np.asarray(triangles, np.int64)
-    out = np.zeros_like(p)
+    if order is not None:
+        t = t[order]
+    vec = np.zeros_like(p)
+    wsum = np.zeros(p.shape[0])
     if t.shape[0] == 0:
-        return np.zeros(p.shape[0])
+        return vec, wsum
     v0, v1, v2 = p[t[:, 0]], p[t[:, 1]], p[t[:, 2]]
 
     def unit(a):
@@ -64,22 +69,33 @@ def normal_sum_magnitude(positions, triangles):
     n = unit(np.cross(v1 - v0, v2 - v0))
     cos = [np.einsum("ij,ij->i", d0, d2), -np.einsum("ij,ij->i", d0, d1), np.einsum("ij,ij->i", d1, d2)]
     for k in range(3):
-        np.add.at(out, t[:, k], n * np.arccos(np.clip(cos[k], -1.0, 1.0))[:, None])
-    return np.linalg.norm(out, axis=1)
+        ang = np.arccos(np.clip(cos[k], -1.0, 1.0))
+        np.add.at(vec, t[:, k], n * ang[:, None])
+        np.add.at(wsum, t[:, k], ang)
+    return vec, wsum
 
 
-# A vertex whose angle-weighted normals (nearly) cancel has no stable
-# direction: the sum's rounding -- the order of the reference's OpenMP
-# atomics, or of the GPU's -- decides it.  Such vertices may differ.
-ILL_CONDITIONED_SUM = 1e-9
+# Rounding in the weighted sum is a few units in the last place of the
+# weights' total W; after normalising by the sum's length |s| that becomes a
+# direction error of about 1e-16 W / |s|.  Vertices whose weighted normals
+# (nearly) cancel are ill-conditioned: the summation order -- the reference's
+# OpenMP atomics or the GPU's -- decides their direction, so the tolerance
+# grows with W / |s| (and is unbounded where s = 0).
+NORMAL_COND_FACTOR = 1e-13
 
 
 def check_normals(got, want, positions, triangles, atol):
-    bad = np.abs(np.asarray(got) - np.asarray(want)).max(1) > atol if len(want) else np.zeros(0, bool)
-    if bad.any():
-        mag = normal_sum_magnitude(positions, triangles)[bad]
-        assert bad.sum() <= max(2, int(1e-5 * len(want))), int(bad.sum())
-        assert np.all(mag < ILL_CONDITIONED_SUM), mag
+    got, want = np.asarray(got), np.asarray(want)
+    if len(want) == 0:
+        return
+    diff = np.abs(got - want).max(1)
+    bad = diff > atol
+    if not bad.any():
+        return
+    vec, wsum = normal_sums(positions, triangles)
+    mag = np.linalg.norm(vec, axis=1)[bad]
+    tol = atol + NORMAL_COND_FACTOR * np.divide(wsum[bad], mag, out=np.full(mag.shape, np.inf), where=mag > 0)
+    assert np.all(diff[bad] <= tol), (int(bad.sum()), diff[bad][diff[bad] > tol][:5], mag[diff[bad] > tol][:5])
 
 
 def fill_counts(n):
@@ -220,3 +236,21 @@ def test_indexed_ring_replay_matches_literal_scan(seed):
     order = rng.permutation(len(edges))
     edges = [edges[i] for i in order]
     assert replay_indexed(edges) == pyoracle.border_rings(edges)
+
+
+def test_normal_tolerance_covers_reordered_sums():
+    """The restatement fed the golden damaged mesh's triangles in other orders
+    (what FP64 atomics do): its normals move only where check_normals'
+    condition-number tolerance allows."""
+    from pathlib import Path
+    g = np.load(Path(__file__).resolve().parent / "golden" / "mesh_post.npz")
+    p, t, n = g["post_pos"], g["post_tris"], g["post_nrm"]
+    rng = np.random.default_rng(0)
+    moved = 0
+    for _ in range(3):
+        perm = rng.permutation(t.shape[0])
+        c, _, n2, _, _ = pyoracle.mesh_postprocess(p, t[perm], min_isle_size=1)
+        assert c["holes"] == 0 and c["isle_vertices"] == 0
+        moved += int((np.abs(n2 - n).max(1) > 1e-12).sum())
+        check_normals(n2, n, p, t, 1e-12)
+    assert moved > 0   # the phenomenon is real on this mesh
