@@ -74,6 +74,35 @@ def test_cone_pruning_cannot_change_sums():
     np.testing.assert_array_equal(a["states"], b["states"])
 
 
+def _with_links(sc, links):
+    return scenes.Scene(sc.pos, sc.nrm, sc.scale, sc.conf, np.ascontiguousarray(links, np.uint32), sc.cams,
+                        sc.name)
+
+
+def test_multiple_camera_links():
+    """K > 1 (MVE captures link up to 5 cameras, Samples.h:311): link l is
+    sample l / K, slot l % K (Occupancy.cpp:250-277), invalid slots
+    (Cameras::INVALID_ID) add nothing, and a repeated link adds its kernels
+    twice."""
+    sc = scenes.sphere_scene(stride=8, width=160, height=120, f=125.0)
+    one = Oracle(sc).build_tree().occupancy(nthreads=1).fields()
+    pad = np.concatenate([sc.links, np.full_like(sc.links, INVALID), np.full_like(sc.links, INVALID)], 1)
+    padded = Oracle(_with_links(sc, pad)).build_tree().occupancy(nthreads=1).fields()
+    for k in ("e_sum", "s_sum", "e_len", "s_len", "prior", "occ"):
+        np.testing.assert_array_equal(padded[k], one[k], err_msg=k)
+    assert padded["cone_count"] == one["cone_count"]
+    dup = np.concatenate([sc.links, sc.links], 1)
+    twice = Oracle(_with_links(sc, dup)).build_tree().occupancy(nthreads=1).fields()
+    for k in ("e_sum", "s_sum", "e_len", "s_len"):
+        np.testing.assert_allclose(twice[k], 2 * one[k], rtol=1e-12, atol=1e-300, err_msg=k)
+    assert twice["cone_count"] == pytest.approx(2 * one["cone_count"], rel=1e-12)
+    np.testing.assert_allclose(twice["prior"], one["prior"], rtol=1e-12, equal_nan=True)
+    # other cameras' links change the field
+    other = np.concatenate([sc.links, (sc.links + 5) % sc.cams.shape[0]], 1)
+    more = Oracle(_with_links(sc, other)).build_tree().occupancy(nthreads=1).fields()
+    assert np.any(more["e_sum"] != one["e_sum"])
+
+
 @pytest.fixture(scope="module")
 def built(tiny_scene):
     o = Oracle(tiny_scene).build_tree()
