@@ -117,7 +117,7 @@ typedef struct {
     uint64_t repaired_leaves;          /* skipped leaves queried after all: they bordered a sign change */
 } tsr_occupancy_counts;
 
-/* The learned pruner (north_star's MLP; no counterpart in the reference).
+/* The learned pruner (no counterpart in the reference).
  * A 10 -> 64 -> 64 -> 2 ReLU MLP over per-leaf features (tsr_occupancy_leaf_features)
  * with two logits: "occupancy > 0" and "near a sign change".  Parameters are
  * FP32, TSR_MLP_PARAMS values in the order W1[10][64], b1[64], W2[64][64],
