@@ -274,3 +274,32 @@ def test_samples_from_depth_meshes():
     a.scales[2] = 0.0
     with pytest.raises(ValueError, match="non-positive"):
         core.Samples.fromDepthMeshes([a], [0])
+
+
+@pytest.mark.parametrize("ending", [files.ENDING_NODES, files.ENDING_LEAVES, files.ENDING_DUAL_CELLS])
+def test_library_survives_byte_flips(ending, tmp_path):
+    """Single flipped bytes anywhere in a file: the load either rejects the
+    file set (TSR_ERR_INVALID_ARG) or, when every check still holds (a flip in
+    a Scope record's padding, say), gets as far as the first device
+    allocation; it never crashes."""
+    import ctypes
+    from tsr_b200 import core
+    g = _golden("sphere_small")
+    s = tree_order_samples(g)
+    prefix = _damaged(tmp_path, "t", lambda n, l, c: None)
+    path = Path(str(prefix) + ending)
+    body = path.read_bytes()
+    rng = np.random.default_rng(len(ending))
+    outcomes = set()
+    for pos in rng.integers(0, len(body), 40):
+        damaged = bytearray(body)
+        damaged[pos] ^= 1 << int(rng.integers(0, 8))
+        path.write_bytes(bytes(damaged))
+        h = ctypes.c_void_p()
+        rc = core.lib.tsr_tree_load(str(prefix).encode(), ctypes.byref(s.view()), None, None, None, ctypes.byref(h))
+        if h.value:   # a GPU machine loaded an equivalent tree
+            core.lib.tsr_tree_free(h)
+        outcomes.add(core.STATUS[rc])
+    path.write_bytes(body)
+    assert outcomes <= {"TSR_ERR_INVALID_ARG", "TSR_ERR_OOM", "TSR_ERR_CUDA", "TSR_OK"}
+    assert "TSR_ERR_INVALID_ARG" in outcomes
