@@ -303,3 +303,41 @@ def test_library_survives_byte_flips(ending, tmp_path):
     path.write_bytes(body)
     assert outcomes <= {"TSR_ERR_INVALID_ARG", "TSR_ERR_OOM", "TSR_ERR_CUDA", "TSR_OK"}
     assert "TSR_ERR_INVALID_ARG" in outcomes
+
+
+def test_numpy_files_round_trip_random_shapes(tmp_path):
+    """write/read of every kind with random sizes, including empty arrays."""
+    rng = np.random.default_rng(9)
+    for trial in range(6):
+        nn, nl, ne, nc = (int(x) for x in rng.integers(0, 50, 4))
+        nodes = {k: rng.integers(0, 2 ** 32, nn, dtype=np.uint64).astype(np.uint32)
+                 for k in ("children", "parents", "counts", "starts")}
+        leaves = dict(scopes=rng.standard_normal((nl, 4)), node_idx=rng.integers(0, 99, nl).astype(np.uint32),
+                      node_to_leaf=rng.integers(0, 99, nn).astype(np.uint32),
+                      nb_offsets=np.sort(rng.integers(0, 99, nl + 1)).astype(np.uint32),
+                      nbs=rng.integers(0, 99, ne).astype(np.uint32))
+        cells = rng.integers(0, 99, (nc, 8)).astype(np.uint32)
+        files.write_tree(tmp_path / ("t%d" % trial), nodes, leaves, cells)
+        n2, l2, c2 = files.read_tree(tmp_path / ("t%d" % trial))
+        for k in nodes:
+            np.testing.assert_array_equal(n2[k], nodes[k])
+        for k in leaves:
+            np.testing.assert_array_equal(l2[k], leaves[k])
+        np.testing.assert_array_equal(c2, cells)
+        fld = {k: rng.standard_normal(nl) for k in files.OCC_FIELDS}
+        fld["states"] = rng.integers(0, 4, nn).astype(np.uint32)
+        fld["cone_count"] = float(rng.random())
+        files.write_occupancy(tmp_path / ("f%d" % trial), fld)
+        f2 = files.read_occupancy(tmp_path / ("f%d" % trial))
+        for k in fld:
+            np.testing.assert_array_equal(f2[k], fld[k])
+        k = int(rng.integers(1, 5))
+        pos, nrm, col = (rng.standard_normal((nl, 3)) for _ in range(3))
+        sc, cf = rng.random(nl), rng.random(nl)
+        links = rng.integers(0, 2 ** 32, (nl, k), dtype=np.uint64).astype(np.uint32)
+        aabb = rng.standard_normal((2, 3))
+        files.write_samples(tmp_path / ("s%d" % trial), pos, nrm, sc, cf, links, aabb, col)
+        d = files.read_samples(tmp_path / ("s%d" % trial))
+        for key, v in (("positions", pos), ("normals", nrm), ("colors", col), ("scales", sc),
+                       ("confidences", cf), ("camera_links", links), ("aabb", aabb)):
+            np.testing.assert_array_equal(d[key], v)
