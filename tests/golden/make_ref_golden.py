@@ -1,0 +1,67 @@
+"""Generates the reference-pinned fixtures tests/golden/ref_*.npz from the
+reference's own hot path (its Scene/Tree and SurfaceExtraction sources built
+unmodified against the project's BaseProject shim: `make -C oracle ref`,
+oracle/refpy.py), run on one thread.
+
+Each fixture holds a seeded scene's samples and cameras and what the
+reference computes for them: the node arrays, the sample permutation, leaf
+scopes, node->leaf links, the neighbour CSR, dual cells, the occupancy field
+(kernel sums, cone lengths, priors, node states, cone count, occupancy of
+every leaf) and the raw DMC mesh.  Scenes: the two golden scenes of
+make_golden.py, a K = 3 capture with invalid and repeated camera links, and a
+small cluttered capture (outliers, confidences in [0.2, 1]).
+
+Usage: python tests/golden/make_ref_golden.py   (needs the reference sources)
+"""
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+
+from oracle import refpy  # noqa: E402
+from tsr_b200 import scenes  # noqa: E402
+
+GOLDEN = Path(__file__).resolve().parent
+INVALID = 0xFFFFFFFF
+
+
+def k3_scene():
+    """The sparse sphere capture with K = 3 links per sample: its own camera,
+    then a random other camera or an invalid slot, then a repeat of the first
+    link or an invalid slot."""
+    sc = scenes.sphere_scene(stride=8, width=160, height=120, f=125.0)
+    rng = np.random.default_rng(21)
+    n, nc = sc.n, sc.cams.shape[0]
+    other = (sc.links[:, 0] + rng.integers(1, nc, n)) % nc
+    s1 = np.where(rng.random(n) < 0.6, other, INVALID).astype(np.uint32)
+    s2 = np.where(rng.random(n) < 0.3, sc.links[:, 0], INVALID).astype(np.uint32)
+    links = np.stack([sc.links[:, 0], s1, s2], 1).astype(np.uint32)
+    return scenes.Scene(sc.pos, sc.nrm, sc.scale, sc.conf, np.ascontiguousarray(links), sc.cams, "sphere_k3")
+
+
+def fixture_scenes():
+    return {
+        "ref_sphere_small": scenes.sphere_scene(stride=6, width=160, height=120, f=125.0),
+        "ref_csg_3k": scenes.csg_scene(seed=3, n_target=3000, width=160, height=120, f=125.0, n_cams=12),
+        "ref_sphere_k3": k3_scene(),
+        "ref_cluttered_2k": scenes.cluttered_scene(seed=2, n_target=2000),
+    }
+
+
+def main():
+    for name, sc in fixture_scenes().items():
+        r = refpy.run(sc, threads=1)
+        out = {k: v for k, v in r.items() if k != "fields" and not k.startswith("samples_")}
+        out.update({"field_" + k: np.asarray(v) for k, v in r["fields"].items()})
+        inputs = dict(in_pos=sc.pos, in_nrm=sc.nrm, in_scale=sc.scale, in_conf=sc.conf, in_links=sc.links,
+                      in_cams=sc.cams)
+        np.savez_compressed(GOLDEN / (name + ".npz"), **inputs, **out)
+        print(name, sc.n, "samples, K =", sc.k, ",", out["children"].shape[0], "nodes,", out["tris"].shape[0],
+              "triangles")
+
+
+if __name__ == "__main__":
+    main()
