@@ -43,6 +43,7 @@ def lib():
         L.tsro_get_sample_depths.argtypes = [P, P]
         L.tsro_occupancy.argtypes = [P, ctypes.c_int, ctypes.c_int]
         L.tsro_occupancy_links.argtypes = [P, ctypes.c_int, ctypes.c_uint64, ctypes.c_uint64]
+        L.tsro_occupancy_update.argtypes = [P, ctypes.c_int, P, ctypes.c_uint32, ctypes.c_int]
         L.tsro_get_occupancy.argtypes = [P, P, P, P, P, P, P, P, P]
         L.tsro_dmc.argtypes = [P]
         L.tsro_set_occupancy.argtypes = [P, P]
@@ -143,6 +144,13 @@ class Oracle:
     def occupancy_links(self, first, count, nthreads=0):
         if lib().tsro_occupancy_links(self.h, nthreads, first, count) != 0:
             raise RuntimeError("oracle occupancy failed")
+        return self
+
+    def update(self, samples, removal, nthreads=1):
+        """Occupancy::addSamples / eraseSamples of tree-order sample indices."""
+        idx = np.ascontiguousarray(samples, np.uint32)
+        if lib().tsro_occupancy_update(self.h, nthreads, _p(idx), idx.shape[0], 1 if removal else 0) != 0:
+            raise RuntimeError("oracle update failed")
         return self
 
     def fields(self):

@@ -133,6 +133,24 @@ int tsrr_run(uint32_t n, uint32_t k, const double *pos, const double *nrm, const
     }
 }
 
+// Occupancy::eraseSamples (removal != 0) or addSamples (Occupancy.h:167-175)
+// of the chosen samples (indices into the reordered samples), then the field
+// saved again as "ref.occupancy" and the occupancy of every leaf.
+int tsrr_update(const uint32_t *samples, uint32_t count, int removal) {
+    QuietCout quiet;
+    try {
+        if (!g_occ) throw std::runtime_error("no field to update");
+        if (removal) g_occ->eraseSamples(samples, count);
+        else g_occ->addSamples(samples, count);
+        g_occ->saveToFile(Storage::Path("ref.occupancy"));
+        for (uint32 l = 0; l < g_occupancy.size(); ++l) g_occupancy[l] = g_occ->getOccupancy(l);
+        return 0;
+    } catch (const std::exception &e) {
+        g_error = e.what();
+        return -1;
+    }
+}
+
 // Bytes the reference's writer saved under `name` ("ref.nodes", "ref.leaves",
 // "ref.dualCells", "ref.occupancy"): the size when dst is null, else copied.
 uint64_t tsrr_file(const char *name, void *dst, uint64_t cap) {

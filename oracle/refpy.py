@@ -46,6 +46,7 @@ def lib():
         L.tsrr_samples.argtypes = [P, P, P, P, P, P]
         L.tsrr_occupancy.argtypes = [P]
         L.tsrr_mesh.argtypes = [P, P, P, P]
+        L.tsrr_update.argtypes = [P, ctypes.c_uint32, ctypes.c_int]
         _lib = L
     return _lib
 
@@ -64,6 +65,35 @@ def _file(name):
 
 SCOPE_DTYPE = np.dtype({"names": ["min", "size", "idx"], "formats": [("<f8", 3), "<f8", "<u4"],
                         "offsets": [0, 24, 32], "itemsize": 40})
+
+
+def _fields():
+    """The field the reference's Occupancy::saveToFile wrote, and
+    getOccupancy of every leaf."""
+    b = _file("ref.occupancy")
+    c = b[:8].view(np.uint32)
+    L, N = int(c[0]), int(c[1])
+    o = 8
+    f = {}
+    for name in ("e_len", "e_sum", "s_len", "s_sum", "prior"):
+        f[name] = b[o:o + 8 * L].view(np.float64).copy()
+        o += 8 * L
+    f["states"] = b[o:o + 4 * N].view(np.uint32).copy()
+    o += 4 * N
+    f["cone_count"] = float(b[o:o + 8].view(np.float64)[0])
+    occ = np.zeros(L)
+    lib().tsrr_occupancy(_p(occ))
+    f["occ"] = occ
+    return f
+
+
+def update(samples, removal):
+    """Occupancy::eraseSamples (removal) / addSamples of tree-order sample
+    indices on the field of the last run; returns the updated field."""
+    idx = np.ascontiguousarray(samples, np.uint32)
+    if lib().tsrr_update(_p(idx), idx.shape[0], 1 if removal else 0) != 0:
+        raise RuntimeError("reference update failed: " + lib().tsrr_last_error().decode())
+    return _fields()
 
 
 def run(scene, params=DEFAULT_PARAMS, stage=2, threads=1, outputs=True):
@@ -109,20 +139,7 @@ def run(scene, params=DEFAULT_PARAMS, stage=2, threads=1, outputs=True):
     out.update(samples_pos=sp, samples_nrm=sn, samples_scale=ss, samples_conf=scf, samples_links=sl,
                permutation=tg)
     if stage >= 1:
-        b = _file("ref.occupancy")
-        c = b[:8].view(np.uint32)
-        L, N = int(c[0]), int(c[1])
-        o = 8
-        f = {}
-        for name in ("e_len", "e_sum", "s_len", "s_sum", "prior"):
-            f[name] = b[o:o + 8 * L].view(np.float64).copy()
-            o += 8 * L
-        f["states"] = b[o:o + 4 * N].view(np.uint32).copy(); o += 4 * N
-        f["cone_count"] = float(b[o:o + 8].view(np.float64)[0])
-        occ = np.zeros(L)
-        lib().tsrr_occupancy(_p(occ))
-        f["occ"] = occ
-        out["fields"] = f
+        out["fields"] = _fields()
     if stage >= 2:
         c = np.zeros(2, np.uint32)
         lib().tsrr_mesh(_p(c), None, None, None)

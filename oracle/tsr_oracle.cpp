@@ -671,8 +671,13 @@ struct tsro_scene {
         }
     }
 
-    // Occupancy.cpp:138-248 for links [first, last)
-    void update_kernels(int type, uint64_t first, uint64_t last, int prune) {
+    // Occupancy.cpp:138-248 for links [first, last), or with `chosen` for the
+    // links of the chosen samples (link l: sample chosen[l / K], slot l % K,
+    // Occupancy.cpp:262-266); removal negates the kernel values, the cone
+    // lengths and the cone count and sets no flags (Occupancy.cpp:210-234,
+    // 335-341).
+    void update_kernels(int type, uint64_t first, uint64_t last, int prune, const uint32_t *chosen = nullptr,
+                        bool removal = false) {
         if (type == EMPTINESS) forward_flag(0, FLAG_SAMPLENESS);
         uint32_t leaf_flag = (type == EMPTINESS) ? FLAG_EMPTINESS : FLAG_SAMPLENESS;
         uint32_t req = (type == EMPTINESS) ? FLAG_SAMPLENESS : 0u;
@@ -682,8 +687,8 @@ struct tsro_scene {
         uint32_t *st = states.data();
 #pragma omp parallel for schedule(dynamic, 128) reduction(+ : count_sum)
         for (int64_t l = (int64_t)first; l < (int64_t)last; ++l) {
-            uint32_t s = (uint32_t)(l / K);
-            uint32_t cam = links[(size_t)l];
+            uint32_t s = chosen ? chosen[l / K] : (uint32_t)(l / K);
+            uint32_t cam = chosen ? links[(size_t)s * K + (size_t)(l % K)] : links[(size_t)l];
             if (cam == INVALID || cam >= C) continue;   // Occupancy.cpp:250-277
             const V3 &cw = cams[cam];
             V3 normal = neg(nrm[s]);
@@ -703,8 +708,8 @@ struct tsro_scene {
             if (cone_degenerated(cone)) continue;
             uint32_t max_depth = MAX_DEPTH_DIFFERENCE + sample_depth(s);   // Occupancy.cpp:518-521
             double c = conf[s];
-            double wlen = c * cone.length;
-            if (type == EMPTINESS) count_sum += c;
+            double wlen = (removal ? -1.0 : 1.0) * c * cone.length;
+            if (type == EMPTINESS) count_sum += removal ? -c : c;
             auto ignored = [&](const Scope &sc, uint32_t depth) {   // ConeNodesChecker.cpp:50-66
                 if (depth > max_depth) return true;
                 if (req != (req & st[sc.idx])) return true;
@@ -715,13 +720,16 @@ struct tsro_scene {
                 V3 center = sc.center();
                 double val;
                 if (!add_kernel(val, center, cone, type == SAMPLENESS, c)) return;
+                if (removal) val = -val;
                 uint32_t leaf = node_to_leaf[sc.idx];
 #pragma omp atomic
                 ks[leaf] += val;
 #pragma omp atomic
                 cl[leaf] += wlen;
+                if (!removal) {
 #pragma omp atomic
-                st[sc.idx] |= leaf_flag;
+                    st[sc.idx] |= leaf_flag;
+                }
             };
             if (!ignored(root, 0)) for_leaves(root, 0, max_depth, ignored, visit);
         }
@@ -800,6 +808,26 @@ struct tsro_scene {
         compute_priors();
         double t3 = now();
         stage[6] = t1 - t0; stage[7] = t2 - t1; stage[8] = t3 - t2;
+        uint32_t L = (uint32_t)leaves.size();
+        occ.resize(L);
+        for (uint32_t l = 0; l < L; ++l) occ[l] = get_occupancy(l);
+        return 0;
+    }
+
+    // Occupancy::addSamples / eraseSamples (Occupancy.h:167-175) ->
+    // onSamplesChanged -> update (Occupancy.cpp:129-136, Occupancy.h:222-227):
+    // both cone passes over the chosen samples' links, then the priors; the
+    // occupancy values follow from the updated sums.
+    int update(int nthreads, const uint32_t *chosen, uint32_t count, bool removal) {
+#ifdef _OPENMP
+        if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+        for (uint32_t i = 0; i < count; ++i)
+            if (chosen[i] >= N) return -1;
+        const uint64_t nl = (uint64_t)count * K;
+        update_kernels(SAMPLENESS, 0, nl, 1, chosen, removal);
+        update_kernels(EMPTINESS, 0, nl, 1, chosen, removal);
+        compute_priors();
         uint32_t L = (uint32_t)leaves.size();
         occ.resize(L);
         for (uint32_t l = 0; l < L; ++l) occ[l] = get_occupancy(l);
@@ -937,6 +965,10 @@ void tsro_get_sample_depths(const tsro_scene *s, uint32_t *d) {
 
 int tsro_occupancy(tsro_scene *s, int nthreads, int prune) {
     try { return s->occupancy(nthreads, prune, 0, (uint64_t)s->N * s->K); } catch (const std::exception &) { return -1; }
+}
+
+int tsro_occupancy_update(tsro_scene *s, int nthreads, const uint32_t *samples, uint32_t count, int removal) {
+    try { return s->update(nthreads, samples, count, removal != 0); } catch (const std::exception &) { return -1; }
 }
 
 int tsro_occupancy_links(tsro_scene *s, int nthreads, uint64_t first, uint64_t count) {

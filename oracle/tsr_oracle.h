@@ -79,6 +79,9 @@ int tsro_occupancy(tsro_scene *s, int nthreads, int prune);
 /* Runs only the links [first, first+count) of both passes; used to time a
  * bounded sample of the field computation.  Returns 0 on success. */
 int tsro_occupancy_links(tsro_scene *s, int nthreads, uint64_t first, uint64_t count);
+/* Occupancy::addSamples / eraseSamples (removal != 0) of samples given by
+ * their tree-order indices, after tsro_occupancy (Occupancy.cpp:129-136). */
+int tsro_occupancy_update(tsro_scene *s, int nthreads, const uint32_t *samples, uint32_t count, int removal);
 void tsro_get_occupancy(const tsro_scene *s, double *e_sum, double *s_sum,
                         double *e_len, double *s_len, double *prior, double *occ,
                         uint32_t *node_states, double *cone_count);

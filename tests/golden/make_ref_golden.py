@@ -10,6 +10,9 @@ scopes, node->leaf links, the neighbour CSR, dual cells, the occupancy field
 every leaf) and the raw DMC mesh.  Scenes: the two golden scenes of
 make_golden.py, a K = 3 capture with invalid and repeated camera links, and a
 small cluttered capture (outliers, confidences in [0.2, 1]).
+ref_update_csg_3k.npz holds the incremental update of the CSG fixture's
+field: Occupancy::eraseSamples of 10 % of the samples (tree-order indices,
+seed 4), then Occupancy::addSamples of the same samples.
 
 Usage: python tests/golden/make_ref_golden.py   (needs the reference sources)
 """
@@ -61,6 +64,22 @@ def main():
         np.savez_compressed(GOLDEN / (name + ".npz"), **inputs, **out)
         print(name, sc.n, "samples, K =", sc.k, ",", out["children"].shape[0], "nodes,", out["tris"].shape[0],
               "triangles")
+    update_fixture()
+
+
+def update_fixture():
+    sc = fixture_scenes()["ref_csg_3k"]
+    refpy.run(sc, threads=1)
+    chosen = np.sort(np.random.default_rng(4).choice(sc.n, size=sc.n // 10, replace=False)).astype(np.uint32)
+    erased = refpy.update(chosen, True)
+    added = refpy.update(chosen, False)
+    out = {"chosen": chosen}
+    out.update({"erased_" + k: np.asarray(v) for k, v in erased.items()})
+    out.update({"added_" + k: np.asarray(v) for k, v in added.items()})
+    inputs = dict(in_pos=sc.pos, in_nrm=sc.nrm, in_scale=sc.scale, in_conf=sc.conf, in_links=sc.links,
+                  in_cams=sc.cams)
+    np.savez_compressed(GOLDEN / "ref_update_csg_3k.npz", **inputs, **out)
+    print("ref_update_csg_3k", chosen.shape[0], "samples erased and added again")
 
 
 if __name__ == "__main__":

@@ -139,3 +139,44 @@ def test_dmc_against_fp64_field(csg_small):
     om = o.dmc()
     diff = (m.cases != om["cases"]).mean()
     assert diff < 5e-3, diff
+
+
+@pytest.fixture(scope="module")
+def c1_scene():
+    """C1 at full size: the unit sphere seen by 24 cameras at 640x480, every
+    3rd pixel (~260k samples)."""
+    from tsr_b200 import scenes
+    return scenes.sphere_scene(stride=3)
+
+
+def test_c1_full_size_against_oracle(c1_scene):
+    """The CPU-runnable configuration at full size: tree bit-exact, the field
+    within the fieldcheck tolerances of the FP64 oracle, and every DMC case
+    code that differs from the FP64 oracle's explained by a counted sign flip
+    of one of its corner leaves."""
+    import os
+
+    from fieldcheck import OUTLIER_FRAC, field_stats, log
+    from tsr_b200 import core
+    o, t, _ = _run(c1_scene)
+    _check_tree(o, t)
+    o.occupancy(nthreads=os.cpu_count() or 1)
+    of = o.fields()
+    g = core.Occupancy(t, core.Cameras(c1_scene.cams))
+    s = field_stats(of, g, t.counts["leaves"])
+    m = g.extractCrust()
+    om = o.dmc()
+    diff = np.nonzero(m.cases != om["cases"])[0]
+    flipped = np.zeros(t.counts["leaves"], bool)
+    flipped[np.nonzero((g.getOccupancy() > 0) != (of["occ"] > 0))[0]] = True
+    cells = t.getDualCells()
+    unexplained = [int(c) for c in diff if not flipped[cells[c]].any()]
+    s.update(case_mismatches=int(diff.size), unexplained_case_mismatches=unexplained[:20],
+             triangles=[int(m.triangles.shape[0]), int(om["tris"].shape[0])])
+    log({"test": "c1_full_size", "samples": c1_scene.n, **s})
+    L = t.counts["leaves"]
+    allowed = max(2, int(OUTLIER_FRAC * L))
+    for k in ("emptiness_sum", "sampleness_sum", "emptiness_length", "sampleness_length", "prior_emptiness"):
+        assert s[k]["outside"] <= allowed, (k, s[k])
+    assert s["sign_flip_count"] <= allowed, s["sign_flips"]
+    assert not unexplained, unexplained[:20]

@@ -19,7 +19,7 @@ from oracle.pyoracle import Oracle
 from tsr_b200 import scenes
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
-FIXTURES = sorted(p.stem for p in GOLDEN.glob("ref_*.npz"))
+FIXTURES = sorted(p.stem for p in GOLDEN.glob("ref_*.npz") if not p.stem.startswith("ref_update"))
 INVALID = 0xFFFFFFFF
 
 
@@ -99,3 +99,16 @@ def test_restatement_matches_live_reference(name):
     ref = {k: v for k, v in r.items() if k != "fields"}
     ref.update({"field_" + k: np.asarray(v) for k, v in r["fields"].items()})
     assert_same(ref, restatement(sc), name)
+
+
+def test_restatement_update_matches_reference():
+    """Occupancy::eraseSamples then addSamples (Occupancy.h:167-175,
+    Occupancy.cpp:129-136) of 10 % of the samples: the restatement's update
+    reproduces the reference's fields bit for bit after each."""
+    g = np.load(GOLDEN / "ref_update_csg_3k.npz")
+    o = Oracle(_scene(g)).build_tree()
+    o.occupancy(nthreads=1)
+    for step, removal in (("erased", True), ("added", False)):
+        f = o.update(g["chosen"], removal, nthreads=1).fields()
+        for k in ("e_sum", "s_sum", "e_len", "s_len", "prior", "occ", "states", "cone_count"):
+            np.testing.assert_array_equal(np.asarray(f[k]), g[step + "_" + k], err_msg="%s %s" % (step, k))
