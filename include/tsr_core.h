@@ -345,6 +345,15 @@ TSR_API tsr_status tsr_occupancy_compute_pruned(const tsr_tree *tree, const tsr_
  * (instrumentation; no counterpart in the reference). */
 TSR_API unsigned long long tsr_kernel_launches(void);
 
+/* Iteration bounds of the tree build (no counterpart in the reference, whose
+ * loops are unbounded): the conflict waves of one sampling round, a loop that
+ * runs on the device inside one cooperative launch and, when it reaches its
+ * bound, stops, records the fact and returns; and the host-side rounds of the
+ * sampling and balancing passes.  A build that reaches either bound returns
+ * TSR_ERR_TIMEOUT and leaves the device usable.  0 restores a default
+ * (2^22 waves, 100000 rounds).  Process-wide; not for calls in flight. */
+TSR_API void tsr_set_iteration_limits(uint32_t max_sampling_waves, uint32_t max_rounds);
+
 /* Wall-clock-free stage timing: CUDA-event milliseconds of the last call on
  * this handle, per stage (see tsr_stage names in the implementation). */
 TSR_API tsr_status tsr_tree_stage_ms(const tsr_tree *tree, float *ms, int n);

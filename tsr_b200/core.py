@@ -17,6 +17,7 @@ Failures raise ``TsrError`` (the reference throws FailureHandling::Exception).
 from __future__ import annotations
 
 import ctypes
+import json
 import os
 from pathlib import Path
 
@@ -88,6 +89,7 @@ _sig = {
     "tsr_tree_build_device": (ctypes.c_int, [_P, _P, _P, _P]),
     "tsr_tree_copy_samples": (ctypes.c_int, [_P, _P, _P, _P, _P, _P]),
     "tsr_kernel_launches": (ctypes.c_ulonglong, []),
+    "tsr_set_iteration_limits": (None, [ctypes.c_uint32, ctypes.c_uint32]),
     "tsr_tree_free": (None, [_P]),
     "tsr_tree_get_counts": (ctypes.c_int, [_P, _P]),
     "tsr_tree_root_scope": (ctypes.c_int, [_P, _P]),
@@ -714,8 +716,19 @@ class Pruner:
     def load(cls, path=None):
         path = Path(path) if path else Path(__file__).resolve().parent / "pruner_weights.npz"
         z = np.load(path)
-        return cls(z["weights"], z["mean"], z["inv_std"], float(z["sign_threshold"]), float(z["band_threshold"]),
+        self = cls(z["weights"], z["mean"], z["inv_std"], float(z["sign_threshold"]), float(z["band_threshold"]),
                    int(z["dilation"]))
+        self.meta = json.loads(str(z["meta"])) if "meta" in z.files else {}
+        self.path = str(path)
+        return self
+
+    def describe(self):
+        """Where the weights came from (the training arguments in their meta)."""
+        a = getattr(self, "meta", {}).get("args", {})
+        if not a:
+            return getattr(self, "path", "in-memory weights")
+        return "%s (trained on %s random CSG scenes of %s samples, the last held back for the thresholds)" % (
+            Path(getattr(self, "path", "")).name, a.get("scenes"), a.get("samples"))
 
     def save(self, path, **extra):
         np.savez(path, weights=self.weights, mean=self.mean, inv_std=self.inv_std,
@@ -737,6 +750,13 @@ class Pruner:
 
 def version():
     return lib.tsr_version().decode()
+
+
+def set_iteration_limits(max_sampling_waves=0, max_rounds=0):
+    """Bounds of the tree build's conflict waves (device) and rounds (host);
+    0 restores the defaults.  A build that reaches one fails with
+    TSR_ERR_TIMEOUT."""
+    lib.tsr_set_iteration_limits(int(max_sampling_waves), int(max_rounds))
 
 
 def kernel_launches():

@@ -17,6 +17,11 @@ static std::atomic<unsigned long long> g_launches{0};
 
 void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
+constexpr uint32_t DEFAULT_SAMPLING_WAVES = 1u << 22, DEFAULT_ROUNDS = 100000;
+static std::atomic<uint32_t> g_limit_waves{DEFAULT_SAMPLING_WAVES}, g_limit_rounds{DEFAULT_ROUNDS};
+uint32_t limit_sampling_waves() { return g_limit_waves.load(std::memory_order_relaxed); }
+uint32_t limit_rounds() { return g_limit_rounds.load(std::memory_order_relaxed); }
+
 void fail(tsr_status st, const std::string &msg) { throw Error{st, msg}; }
 
 void check_cuda(cudaError_t e, const char *what) {
@@ -167,6 +172,11 @@ tsr_status tsr_tree_build_device(const tsr_samples_view *samples, const tsr_para
 }
 
 unsigned long long tsr_kernel_launches(void) { return g_launches.load(std::memory_order_relaxed); }
+
+void tsr_set_iteration_limits(uint32_t max_sampling_waves, uint32_t max_rounds) {
+    tsr::g_limit_waves.store(max_sampling_waves ? max_sampling_waves : tsr::DEFAULT_SAMPLING_WAVES);
+    tsr::g_limit_rounds.store(max_rounds ? max_rounds : tsr::DEFAULT_ROUNDS);
+}
 
 void tsr_tree_free(tsr_tree *tree) { delete tree; }
 

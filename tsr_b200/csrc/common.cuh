@@ -33,6 +33,10 @@ struct Error {
 
 [[noreturn]] void fail(tsr_status st, const std::string &msg);
 void note_launch();   // counts this library's kernel launches (instrumentation)
+// Iteration bounds of the tree build (tsr_set_iteration_limits): conflict
+// waves per sampling round (a device-side loop) and host rounds.
+uint32_t limit_sampling_waves();
+uint32_t limit_rounds();
 void check_cuda(cudaError_t e, const char *what);
 #define TSR_CUDA(call) ::tsr::check_cuda((call), #call)
 

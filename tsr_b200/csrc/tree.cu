@@ -1163,8 +1163,12 @@ void build_tree(tsr_tree &t, const tsr_samples_view &sv, bool on_device) {
         const double margin = 1e-12 * (std::max(std::max(std::fabs(root.mn.x), std::fabs(root.mn.y)),
                                                  std::fabs(root.mn.z)) + 2.0 * root.size);
         float eval_ms = 0, resolve_ms = 0;
-        cudaEvent_t e0, e1, e2;
-        TSR_CUDA(cudaEventCreate(&e0)); TSR_CUDA(cudaEventCreate(&e1)); TSR_CUDA(cudaEventCreate(&e2));
+        struct Events {   // destroyed on every exit, a failed round's included
+            cudaEvent_t e[3] = {nullptr, nullptr, nullptr};
+            ~Events() { for (cudaEvent_t x : e) if (x) cudaEventDestroy(x); }
+        } ev;
+        for (cudaEvent_t &x : ev.e) TSR_CUDA(cudaEventCreate(&x));
+        cudaEvent_t e0 = ev.e[0], e1 = ev.e[1], e2 = ev.e[2];
         unsigned coop_grid = 1;
         {
             int dev = 0, sms = 0, per_sm = 0;
@@ -1173,8 +1177,9 @@ void build_tree(tsr_tree &t, const tsr_samples_view &sv, bool on_device) {
             TSR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_waves_coop, 256, 0));
             coop_grid = (unsigned)(sms * (per_sm > 0 ? per_sm : 1));
         }
+        const uint32_t max_waves_used = limit_sampling_waves();
         while (m > 0) {
-            if (++rounds > 100000) fail(TSR_ERR_TIMEOUT, "sampling rounds did not converge");
+            if (++rounds > limit_rounds()) fail(TSR_ERR_TIMEOUT, "sampling rounds did not converge");
             NV v = view(S);
             DBuf<uint8_t> status(m, st);
             DBuf<uint32_t> unres(m, st), witness(m, st), dleaf(m, st);
@@ -1210,7 +1215,7 @@ void build_tree(tsr_tree &t, const tsr_samples_view &sv, bool on_device) {
                 TSR_CUDA(cudaMemcpyAsync(front.p, writers.p, (size_t)nwri * 4, cudaMemcpyDeviceToDevice, st));
                 DBuf<uint32_t> ctr(4, st);
                 ctr.zero();
-                uint32_t max_waves = 1u << 22;
+                uint32_t max_waves = max_waves_used;
                 uint32_t *fp = front.p, *np = next.p, *tp = touched.p, *kp = keys.p, *dp = dleaf.p, *mp = mark.p;
                 uint32_t *slp = seg_lo.p, *shp = seg_hi.p, *blp = by_leaf.p, *up = unres.p, *cp = ctr.p;
                 uint32_t *wp = waves_total.p;
@@ -1228,7 +1233,16 @@ void build_tree(tsr_tree &t, const tsr_samples_view &sv, bool on_device) {
             k_sampling_apply<<<grid_for(m, 128), 128, 0, st>>>(m, keys.p, status.p, unres.p, dleaf.p, v, root, pos.p,
                                                               nrm.p, scale.p, h_svo, nsplit.p, nullptr, 0, 0, derr.p); ::tsr::note_launch();
             exclusive_scan(nsplit.p, base.p, m + 1, st);
-            uint32_t total = read_scalar(base.p + m, st);
+            // the split total, and whether the waves ran out of their bound:
+            // then the round's conflicts are unresolved and nothing is applied
+            uint32_t total = 0;
+            int round_err = 0;
+            TSR_CUDA(cudaMemcpyAsync(&total, base.p + m, 4, cudaMemcpyDeviceToHost, st));
+            TSR_CUDA(cudaMemcpyAsync(&round_err, derr.p, 4, cudaMemcpyDeviceToHost, st));
+            TSR_CUDA(cudaStreamSynchronize(st));
+            if (round_err == 7)
+                fail(TSR_ERR_TIMEOUT, "sampling conflict resolution exceeded its bound of " +
+                                          std::to_string(max_waves_used) + " waves in round " + std::to_string(rounds));
             float a = 0, b = 0;
             TSR_CUDA(cudaEventElapsedTime(&a, e0, e1));
             TSR_CUDA(cudaEventElapsedTime(&b, e1, e2));
@@ -1258,7 +1272,6 @@ void build_tree(tsr_tree &t, const tsr_samples_view &sv, bool on_device) {
             std::swap(keys, keys2);
             m = m2;
         }
-        cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(e2);
         t.sampling_rounds = rounds;
         t.stage_ms[6] = eval_ms;
         t.stage_ms[7] = resolve_ms;
@@ -1282,7 +1295,7 @@ void build_tree(tsr_tree &t, const tsr_samples_view &sv, bool on_device) {
         split_flag.zero();
         DBuf<uint32_t> counters(2, st);
         for (int round = 0;; ++round) {
-            if (round > 100000) fail(TSR_ERR_TIMEOUT, "balancing did not converge");
+            if ((uint32_t)round > limit_rounds()) fail(TSR_ERR_TIMEOUT, "balancing did not converge");
             NV v = view(S);
             DBuf<uint32_t> split_list(m * 6 < S.count ? m * 6 : S.count, st), again(m, st);
             counters.zero();
