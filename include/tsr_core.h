@@ -185,8 +185,9 @@ TSR_API tsr_status tsr_tree_root_scope(const tsr_tree *tree, double min_xyz_size
  * that up (address look-up, which may load the library's device code), so
  * make it before any stream capture.  Calls on one device share the array:
  * calls that may overlap in time race, so order them.  count must be
- * 1 .. 2^32 - 1 (TSR_ERR_OVERFLOW_U32 above); pointers must be 8-byte aligned
- * memory of the current device. */
+ * 1 .. 2^31 - 1, the tree build's limit (TSR_ERR_OVERFLOW_U32 above); pointers
+ * must be 8-byte aligned memory of the current device.  The root cube follows
+ * the build's arithmetic for every input, NaN and negative extents included. */
 TSR_API tsr_status tsr_samples_root_scope_noalloc(uint64_t count, const double *positions,
                                                   const double *scales, const tsr_params *params,
                                                   double *out_min_xyz_size, void *cuda_stream);

@@ -99,8 +99,8 @@ k_root_scope_noalloc(uint64_t n, const double *pos, const double *scale, double 
         }
     block_box(w, sm);
     if (threadIdx.x == 0) {
-        double size = 0;
-        for (int j = 0; j < 3; ++j) size = dmax_(size, dsub(w[3 + j], w[j]));
+        // the build's root_from_aabb: max(max(extent x, extent y), extent z)
+        const double size = dmax_(dmax_(dsub(w[3], w[0]), dsub(w[4], w[1])), dsub(w[5], w[2]));
         double half = dmul(size, 0.5);
         for (int j = 0; j < 3; ++j) out[j] = dsub(dmul(dadd(w[j], w[3 + j]), 0.5), half);
         out[3] = size;
@@ -150,8 +150,8 @@ void root_scope_noalloc(uint64_t count, const double *positions, const double *s
                         double *out_min_xyz_size, cudaStream_t st) {
     if (!positions || !scales || !out_min_xyz_size) fail(TSR_ERR_INVALID_ARG, "null argument");
     if (count == 0) fail(TSR_ERR_INVALID_ARG, "no samples to compute a root scope for");
-    if (count > 0xFFFFFFFFull)
-        fail(TSR_ERR_OVERFLOW_U32, "sample count above the 2^32 - 1 limit of the sample index space");
+    if (count * 2 >= (uint64_t)INVALID)   // the tree build's limit (two sides per sample)
+        fail(TSR_ERR_OVERFLOW_U32, "sample count above the tree build's limit of 2^31 - 1");
     if (!(h_svo > 0)) fail(TSR_ERR_INVALID_ARG, "parameters must be positive");
     if (((uintptr_t)positions | (uintptr_t)scales | (uintptr_t)out_min_xyz_size) & 7)
         fail(TSR_ERR_INVALID_ARG, "arrays must be 8-byte aligned doubles");
