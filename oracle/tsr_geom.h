@@ -4,7 +4,8 @@
  * Vector arithmetic and the geometry predicates the reference's hot path calls.
  * The predicates marked "BaseProject" live in a library that is not part of the
  * reference tree; they are restated here from their call sites and comments
- * (parity at that boundary is unpinned).  Operation order is fixed so that the
+ * (parity at that boundary is unpinned; the reference build's shim,
+ * oracle/ref_shim/, calls these same functions).  Operation order is fixed so that the
  * GPU tree build, which repeats these expressions in FP64, rounds identically.
  */
 #ifndef TSR_ORACLE_GEOM_H

@@ -6,8 +6,14 @@
  * SurfaceReconstruction/SurfaceReconstruction/ in the reference.
  *
  * Real = double.  Built with -ffp-contract=off so every expression rounds
- * exactly as written; the GPU tree build uses the same operation order in
- * FP64 (nvcc -fmad=false) so that topology decisions agree bit for bit.
+ * exactly as written; the GPU tree build evaluates the same expressions in
+ * the same operation order with explicitly round-to-nearest FP64 intrinsics
+ * (__dadd_rn, __dmul_rn, ...; tsr_b200/csrc/common.cuh), which the compiler
+ * never fuses, so that topology decisions agree bit for bit.
+ *
+ * Pinned to the reference: tests/test_ref_pin.py compares every tree,
+ * field and DMC array of this restatement with the reference's own sources
+ * built against the BaseProject shim (oracle/ref_driver.cpp, `make ref`).
  */
 #include "tsr_oracle.h"
 #include "tsr_geom.h"

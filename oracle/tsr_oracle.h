@@ -14,19 +14,18 @@
  * reference).  Each function in tsr_oracle.cpp cites the file:line it follows.
  *
  * Parity pinning: the reference has no tests, golden vectors or fixtures for
- * this path, and its geometry helpers (BaseProject's ObliqueCircularCone,
- * intersectAABBWithSphere, intersectAABBWithLineSegment, Plane, EPSILON) are
- * not in the reference tree.  Those helpers are restated here from their call
- * sites; PARITY UNPINNED: the reference's own sources cannot be compiled
- * here (they need the absent BaseProject library and its cmake build), so no
- * reference-produced output backs this restatement.  What pins it instead is
- * structural: the tests check the restatement's invariants (every sample
- * inside its container, consistent parent/child links, the block-DFS node
- * layout, leaves partitioning the root with the depth-difference balance,
- * dual cells built from existing leaves, the Marching Cubes tables, well
- * formed meshes, the round schedule equal to the sequential sampling pass,
- * cone pruning leaving the kernel sums unchanged) and replay its committed
- * golden fixtures.
+ * this path, so this restatement is pinned against the reference's own code:
+ * `make -C oracle ref` compiles the reference's Scene/Tree and
+ * SurfaceExtraction sources unmodified against a project-written shim of the
+ * absent BaseProject headers (oracle/ref_shim/), and tests/test_ref_pin.py
+ * requires every array of this restatement -- node arrays, permutation,
+ * leaves, neighbours, dual cells, the FP64 field, the incremental update and
+ * the raw DMC mesh -- to equal the reference's bit for bit, on committed
+ * reference-made fixtures (tests/golden/ref_*.npz) and on live runs.  What
+ * stays unpinned is BaseProject itself: its geometry helpers
+ * (ObliqueCircularCone, intersectAABBWithSphere, intersectAABBWithLineSegment,
+ * Plane, EPSILON, REAL_MAX) are restated from their call sites, and the shim
+ * uses these same restatements.
  */
 #ifndef TSR_ORACLE_H
 #define TSR_ORACLE_H
