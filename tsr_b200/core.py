@@ -727,8 +727,10 @@ class Pruner:
         a = getattr(self, "meta", {}).get("args", {})
         if not a:
             return getattr(self, "path", "in-memory weights")
+        n = a.get("samples")
+        size = str(n) if n else "%s-%s" % (a.get("samples_min"), a.get("samples_max"))
         return "%s (trained on %s random CSG scenes of %s samples, the last held back for the thresholds)" % (
-            Path(getattr(self, "path", "")).name, a.get("scenes"), a.get("samples"))
+            Path(getattr(self, "path", "")).name, a.get("scenes"), size)
 
     def save(self, path, **extra):
         np.savez(path, weights=self.weights, mean=self.mean, inv_std=self.inv_std,

@@ -14,7 +14,7 @@ the other leaves a confident but wrong sign.  The pruned field
 network places away from a sign change (plus one ring of face neighbours)
 and whose sign it is sure of.
 
-    python -m tsr_b200.pruner --scenes 8 --samples 1000000 --out tsr_b200/pruner_weights.npz
+    python -m tsr_b200.pruner --scenes 50 --out tsr_b200/pruner_weights.npz
 
 The committed ``pruner_weights.npz`` was produced by that command (its
 ``meta`` entry records the arguments and the training statistics).
@@ -47,7 +47,12 @@ def labels(occupancy, leaves):
 
 
 def scene_rows(scene, params=None):
-    """Features and labels of every leaf of one scene's plain field."""
+    """Features and labels of every leaf of one scene's plain field (a host
+    Scene, a DeviceScene, or a callable making either)."""
+    if callable(scene):
+        scene = scene()
+    if hasattr(scene, "host"):
+        scene = scene.host()
     samples = core.Samples.from_scene(scene)
     tree = core.Tree(samples, params, reorder_samples=False)
     occ = core.Occupancy(tree, core.Cameras(scene.cams), params)
@@ -205,8 +210,12 @@ def judge(tree, cams, pruner, params=None, stream=None):
 
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
-    ap.add_argument("--scenes", type=int, default=8, help="random CSG scenes (the last one is held back)")
-    ap.add_argument("--samples", type=int, default=1_000_000)
+    ap.add_argument("--scenes", type=int, default=50, help="random CSG scenes (the last one is held back)")
+    ap.add_argument("--samples", type=int, default=None, help="samples per scene (default: uniform in "
+                    "--samples-min .. --samples-max per scene)")
+    ap.add_argument("--samples-min", type=int, default=2_000_000)
+    ap.add_argument("--samples-max", type=int, default=4_000_000)
+    ap.add_argument("--host-scenes", action="store_true", help="render the scenes with numpy on the host")
     ap.add_argument("--epochs", type=int, default=4)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--miss", type=float, default=1e-3)
@@ -214,11 +223,19 @@ def main():
     ap.add_argument("--out", default="pruner_weights.npz")
     a = ap.parse_args()
     from . import scenes
-    t0 = time.time()
-    sc = [scenes.random_csg_scene(seed=1 + i, n_target=a.samples) for i in range(a.scenes)]
-    print("scenes generated in %.1f s" % (time.time() - t0), flush=True)
-    pruner, stats = fit(sc, epochs=a.epochs, seed=a.seed, miss=a.miss, dilation=a.dilation)
+    rng = np.random.default_rng(a.seed)
+    sizes = [a.samples or int(rng.integers(a.samples_min, a.samples_max + 1)) for _ in range(a.scenes)]
+
+    def maker(i, n):
+        # scenes are made one at a time, when their rows are taken
+        if a.host_scenes:
+            return lambda: scenes.random_csg_scene(seed=1 + i, n_target=n)
+        return lambda: scenes.random_csg_scene_device(1 + i, n, 1600, 1200, 1200.0)
+
+    pruner, stats = fit([maker(i, n) for i, n in enumerate(sizes)], epochs=a.epochs, seed=a.seed, miss=a.miss,
+                        dilation=a.dilation)
     stats["args"] = vars(a)
+    stats["samples_per_scene"] = sizes
     print(json.dumps(stats), flush=True)
     pruner.save(a.out, meta=np.array(json.dumps(stats)))
 
