@@ -151,6 +151,17 @@ __device__ __forceinline__ bool separated_at(const ConeF &c, float te, F3 q, flo
 }
 
 constexpr int PT_BLOCK = 128;
+// Resident blocks per SM the persistent traversals are compiled for (the
+// register budget: 65536 / (128 threads x blocks)).
+#ifndef TSR_CONE_E_BLOCKS
+#define TSR_CONE_E_BLOCKS 6
+#endif
+#ifndef TSR_CONE_S_BLOCKS
+#define TSR_CONE_S_BLOCKS 5
+#endif
+#ifndef TSR_PRIOR_BLOCKS
+#define TSR_PRIOR_BLOCKS 1
+#endif
 
 // ------------------------------------------- block-expansion cone traversal
 // Thread-per-link depth-first traversal (the per-link LeavesIterator with a
@@ -365,7 +376,7 @@ __global__ void __launch_bounds__(128) k_link_setup(uint64_t nlinks, const uint3
 }
 
 template <int TYPE>
-__global__ void __launch_bounds__(PT_BLOCK, (TYPE == 0) ? 6 : 5) k_cone_x(uint64_t nlinks, const LinkRec *links,
+__global__ void __launch_bounds__(PT_BLOCK, (TYPE == 0) ? TSR_CONE_E_BLOCKS : TSR_CONE_S_BLOCKS) k_cone_x(uint64_t nlinks, const LinkRec *links,
                                                                          TreeIn tr, const uint2 *rec,
                                                                          float root_size_f, double *ksum,
                                                                          double *clen, unsigned long long *accepted,
@@ -638,7 +649,7 @@ __device__ inline bool box_inside_sphere(const D3 &mn, double sz, const D3 &c, d
 // 64-byte line and their FP64 boxes are derived from the parent's corner with
 // the tree build's own recurrence (child_coords, exact), so no node geometry
 // is loaded inside the loop.
-__global__ void __launch_bounds__(PT_BLOCK) k_priors_x(uint32_t nl, uint32_t nn, const uint32_t *list,
+__global__ void __launch_bounds__(PT_BLOCK, TSR_PRIOR_BLOCKS) k_priors_x(uint32_t nl, uint32_t nn, const uint32_t *list,
                                                       const uint32_t *leaf_node, const D3 *leaf_min,
                                                       const uint8_t *depth, const D3 *nmin, const uint2 *rec,
                                                       const double2 *psum, double root_size, double rel_radius,
