@@ -15,7 +15,7 @@ KSUM_RTOL = 2e-4          # kernel sums, per leaf, relative to the leaf's value
 KSUM_ATOL_REL = 1e-6      # ... plus this fraction of the largest sum
 LEN_OUTLIER_FRAC = 1e-3   # cone-length sums may differ by whole terms where a
                           # kernel value sits on the EPSILON acceptance threshold
-PRIOR_ATOL = 1e-4
+PRIOR_ATOL = 1e-4         # see fieldcheck.py: one threshold leaf's length term, measured 1.2e-5
 SIGN_FLIP_FRAC = 1e-3     # leaves whose occupancy sign differs
 
 
@@ -78,29 +78,28 @@ def _field_errors(of, g):
 
 
 def _check_field(scene, o, t):
+    from fieldcheck import field_stats, log
     from tsr_b200 import core
     o.occupancy()
     of = o.fields()
     g = core.Occupancy(t, core.Cameras(scene.cams))
     assert g.field("cone_count") == pytest.approx(of["cone_count"], rel=1e-12)
-    errs = _field_errors(of, g)
     L = t.counts["leaves"]
+    allowed = max(2, int(LEN_OUTLIER_FRAC * L))
+    errs = _field_errors(of, g)
     for name, e in errs.items():
-        assert e["bad"] <= max(2, int(LEN_OUTLIER_FRAC * L)), (name, e)
-    for name, key in [("emptiness_length", "e_len"), ("sampleness_length", "s_len")]:
-        a, b = g.field(name), of[key]
-        bad = np.abs(a - b) > 1e-4 * np.abs(b) + 1e-9 * np.abs(b).max()
-        assert bad.sum() <= max(2, int(LEN_OUTLIER_FRAC * L)), (name, int(bad.sum()))
+        assert e["bad"] <= allowed, (name, e)
+    s = field_stats(of, g, L)
+    log({"test": "field_vs_oracle", "scene": getattr(scene, "name", ""), **s})
+    for k in ("emptiness_length", "sampleness_length"):
+        assert s[k]["outside"] <= allowed, (k, s[k])
+    # priors within PRIOR_ATOL where a threshold leaf's length term differs, exact otherwise
+    assert s["prior_emptiness"]["outside"] == 0, s["prior_emptiness"]
+    assert s["prior_emptiness"]["max_abs"] < PRIOR_ATOL, s["prior_emptiness"]
+    assert s["prior_emptiness"]["nan_mismatch"] <= allowed
     st = g.getNodeStates()
-    assert (st != of["states"]).sum() <= max(2, int(LEN_OUTLIER_FRAC * L))
-    pr = g.getPriorForEmptiness()
-    both = np.isfinite(pr) & np.isfinite(of["prior"])
-    assert (np.isfinite(pr) == np.isfinite(of["prior"])).mean() > 1 - LEN_OUTLIER_FRAC
-    assert np.abs(pr[both] - of["prior"][both]).max() < 5e-2
-    assert (np.abs(pr[both] - of["prior"][both]) > PRIOR_ATOL).mean() < LEN_OUTLIER_FRAC
-    occ_g, occ_o = g.getOccupancy(), of["occ"]
-    flips = ((occ_g > 0) != (occ_o > 0)).sum()
-    assert flips <= max(2, SIGN_FLIP_FRAC * L), flips
+    assert (st != of["states"]).sum() <= allowed
+    assert s["sign_flip_count"] <= max(2, SIGN_FLIP_FRAC * L), s["sign_flips"]
     return g, of
 
 
@@ -130,15 +129,19 @@ def test_dmc_bit_exact_on_gpu_field(tiny_scene):
 
 
 def test_dmc_against_fp64_field(csg_small):
-    """Case codes against the oracle's own FP64 field: differences come only
-    from sign flips of the FP32 field and are counted."""
-    from tsr_b200 import core
+    """Case codes against the oracle's own FP64 field: every cell whose case
+    differs has a corner leaf whose sign flipped (counted), and none other."""
     o, t, _ = _run(csg_small)
     g, of = _check_field(csg_small, o, t)
     m = g.extractCrust()
     om = o.dmc()
-    diff = (m.cases != om["cases"]).mean()
-    assert diff < 5e-3, diff
+    diff = np.nonzero(m.cases != om["cases"])[0]
+    flipped = (g.getOccupancy() > 0) != (of["occ"] > 0)
+    cells = t.getDualCells()
+    unexplained = [int(c) for c in diff if not flipped[cells[c]].any()]
+    assert not unexplained, unexplained[:20]
+    if not flipped.any():
+        np.testing.assert_array_equal(m.cases, om["cases"])
 
 
 @pytest.fixture(scope="module")
@@ -176,7 +179,8 @@ def test_c1_full_size_against_oracle(c1_scene):
     log({"test": "c1_full_size", "samples": c1_scene.n, **s})
     L = t.counts["leaves"]
     allowed = max(2, int(OUTLIER_FRAC * L))
-    for k in ("emptiness_sum", "sampleness_sum", "emptiness_length", "sampleness_length", "prior_emptiness"):
+    for k in ("emptiness_sum", "sampleness_sum", "emptiness_length", "sampleness_length"):
         assert s[k]["outside"] <= allowed, (k, s[k])
+    assert s["prior_emptiness"]["outside"] == 0, s["prior_emptiness"]
     assert s["sign_flip_count"] <= allowed, s["sign_flips"]
     assert not unexplained, unexplained[:20]

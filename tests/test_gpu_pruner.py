@@ -25,8 +25,10 @@ def heldout():
 def test_pruned_field_matches_plain_mesh_with_less_work(heldout):
     from tsr_b200 import core, pruner
     tree, cams = heldout
+    from fieldcheck import log
     j = pruner.judge(tree, cams, core.Pruner.load())
     saved = 1.0 - j["visited"]["visited_priors"][1] / j["visited"]["visited_priors"][0]
+    log({"test": "pruner_judge", "prior_work_saved": saved, **j})
     assert j["case_agreement"] >= MIN_CASE_AGREEMENT, j
     assert j["vertex_hausdorff"] <= MAX_HAUSDORFF_LEAVES * j["finest_leaf_size"], j
     assert saved >= MIN_PRIOR_WORK_SAVED, j

@@ -65,8 +65,9 @@ def test_gpu_field_matches_reference(name):
     log({"test": "field_vs_reference", "fixture": name, **s})
     L = t.counts["leaves"]
     allowed = max(2, int(OUTLIER_FRAC * L))
-    for k in ("emptiness_sum", "sampleness_sum", "emptiness_length", "sampleness_length", "prior_emptiness"):
+    for k in ("emptiness_sum", "sampleness_sum", "emptiness_length", "sampleness_length"):
         assert s[k]["outside"] <= allowed, (k, s[k])
+    assert s["prior_emptiness"]["outside"] == 0, s["prior_emptiness"]
     assert s["prior_emptiness"]["nan_mismatch"] <= allowed, s["prior_emptiness"]
     assert s["cone_count_rel"] < 1e-12
     assert s["sign_flip_count"] <= allowed, s["sign_flips"]
@@ -111,7 +112,8 @@ def test_gpu_update_matches_reference():
         ref = {k[len(step) + 1:]: g[k] for k in g.files if k.startswith(step + "_")}
         s = field_stats(ref, occ, t.counts["leaves"])
         log({"test": "update_vs_reference", "step": step, **s})
-        for k in ("emptiness_sum", "sampleness_sum", "emptiness_length", "sampleness_length", "prior_emptiness"):
+        for k in ("emptiness_sum", "sampleness_sum", "emptiness_length", "sampleness_length"):
             assert s[k]["outside"] <= allowed, (step, k, s[k])
+        assert s["prior_emptiness"]["outside"] == 0, (step, s["prior_emptiness"])
         assert s["sign_flip_count"] <= allowed, (step, s["sign_flips"])
         assert s["cone_count_rel"] < 1e-12

@@ -227,10 +227,15 @@ def main():
     sizes = [a.samples or int(rng.integers(a.samples_min, a.samples_max + 1)) for _ in range(a.scenes)]
 
     def maker(i, n):
-        # scenes are made one at a time, when their rows are taken
+        # scenes are made one at a time, when their rows are taken; every
+        # third training scene also has 5 % outliers and confidences in
+        # [0.2, 1] (the held-back last scene is clean)
         if a.host_scenes:
             return lambda: scenes.random_csg_scene(seed=1 + i, n_target=n)
-        return lambda: scenes.random_csg_scene_device(1 + i, n, 1600, 1200, 1200.0)
+        noisy = i % 3 == 2 and i != a.scenes - 1
+        return lambda: scenes.random_csg_scene_device(1 + i, n, 1600, 1200, 1200.0,
+                                                      outlier_frac=0.05 if noisy else 0.0,
+                                                      conf_range=(0.2, 1.0) if noisy else (1.0, 1.0))
 
     pruner, stats = fit([maker(i, n) for i, n in enumerate(sizes)], epochs=a.epochs, seed=a.seed, miss=a.miss,
                         dilation=a.dilation)

@@ -716,16 +716,19 @@ def _random_csg_prims(rng, n_prims):
     return prims
 
 
-def random_csg_scene_device(seed, n_target, width, height, f, device="cuda"):
+def random_csg_scene_device(seed, n_target, width, height, f, device="cuda", outlier_frac=0.0,
+                            conf_range=(1.0, 1.0)):
     """``random_csg_scene`` rendered on the device: the same primitives and
-    cameras (drawn from the same numpy generator), other noise draws."""
+    cameras (drawn from the same numpy generator), other noise draws;
+    optionally with outliers and varying confidences."""
     rng = np.random.default_rng(1000 + seed)
     n_prims = int(rng.integers(3, 9))
     prims = _random_csg_prims(rng, n_prims)
     n_cams = int(rng.integers(64, 161))
     cams = _random_cams(rng, n_cams, 1.5, 8.0)
     return render_device(prims, cams, width, height, f, 0.005, 8.0, seed=7919 * (seed + 1), target=n_target,
-                         name="random_csg_%d" % seed, device=device)
+                         name="random_csg_%d" % seed, device=device, outlier_frac=outlier_frac,
+                         conf_range=conf_range)
 
 
 def csg_scene_device(seed=0, n_target=4_000_000, width=1280, height=960, f=600.0, n_cams=120, device="cuda"):
