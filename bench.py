@@ -556,7 +556,8 @@ def our_arm(args):
             "value": world_samples * args.steps / t_pruned, "unit": UNIT, "ms_per_step": 1e3 * t_pruned / args.steps,
             "step_ms": [round(x, 3) for x in p_step_ms],
             "speedup_vs_plain": t_value / t_pruned,
-            "skipped_prior_queries": poc.pruned_leaves, "repaired_leaves": poc.repaired_leaves, "leaves": int(Nl),
+            "skipped_prior_queries": poc.pruned_leaves, "repaired_leaves": poc.repaired_leaves,
+            "certified_skips": poc.certified_leaves, "leaves": int(Nl),
             "stage_ms": {k: round(float(v), 3) for k, v in zip(names, pstage / args.steps) if k},
             "judge": {"sign_agreement": j["sign_agreement"], "case_agreement": j["case_agreement"],
                       "vertex_hausdorff": j["vertex_hausdorff"], "finest_leaf_size": j["finest_leaf_size"],

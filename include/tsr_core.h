@@ -115,6 +115,7 @@ typedef struct {
     uint64_t visited_priors;           /* tree nodes classified by the prior sphere queries */
     uint64_t pruned_leaves;            /* prior queries the pruned field skipped (0 for the plain field) */
     uint64_t repaired_leaves;          /* skipped leaves queried after all: they bordered a sign change */
+    uint64_t certified_leaves;         /* skip candidates whose sign bounds of their prior proved */
 } tsr_occupancy_counts;
 
 /* The learned pruner (no counterpart in the reference).
@@ -332,12 +333,17 @@ TSR_API tsr_status tsr_mlp_infer_bf16(const float *x, uint32_t n, const float *p
 /* The pruned field: like tsr_occupancy_compute (both cone passes exact), but
  * the prior query -- the most expensive per-leaf step -- runs only for
  * reliable leaves (E + S >= confidenceThreshold) that the pruner places near
- * a sign change (or within `dilation` rings of face neighbours of one) or
- * whose sign it is not sure of; E == 0 or S == 0 fixes the sign without a
- * prior.  A skipped reliable leaf takes the pruner's sign, with the value
- * 0.5 (S - E) / coneCount when positive; its prior reads NaN.  Skipped
- * leaves that then border a leaf of the other sign are queried after all,
- * until none does, so every leaf on a sign change has its exact value. */
+ * a sign change (or within `dilation` rings of face neighbours of one), whose
+ * sign it is not sure of, or whose sign cannot be certified; E == 0 or
+ * S == 0 fixes the sign without a prior.  Every other reliable leaf gets a
+ * cheaper bounds query (the prior's sphere query stopped at nodes of the
+ * leaf's size, their subtrees counted as undecided), and is skipped only when
+ * the bounds prove its sign ((1 - p) S > p E for every p in them, or for
+ * none); it then takes that sign, with the value 0.5 (S - E) / coneCount
+ * when positive, and its prior reads NaN.  Skipped leaves that border a leaf
+ * of the other sign are queried after all, until none does.  So every sign
+ * is the plain field's, and every leaf on a sign change has its exact value:
+ * the DMC mesh equals the plain field's. */
 TSR_API tsr_status tsr_occupancy_compute_pruned(const tsr_tree *tree, const tsr_cameras_view *cameras,
                                                 const tsr_params *params, const tsr_pruner *pruner,
                                                 void *cuda_stream, tsr_occupancy **out_occupancy);

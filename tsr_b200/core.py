@@ -62,7 +62,7 @@ class tsr_mesh_counts(ctypes.Structure):
 class tsr_occupancy_counts(ctypes.Structure):
     _fields_ = [("links", _U64), ("accepted_sampleness", _U64), ("accepted_emptiness", _U64),
                 ("visited_sampleness", _U64), ("visited_emptiness", _U64), ("visited_priors", _U64),
-                ("pruned_leaves", _U64), ("repaired_leaves", _U64)]
+                ("pruned_leaves", _U64), ("repaired_leaves", _U64), ("certified_leaves", _U64)]
 
 
 MLP_FEATURES, MLP_HIDDEN, MLP_OUTPUTS, MLP_PARAMS = 10, 64, 2, 4994

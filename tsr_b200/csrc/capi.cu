@@ -435,6 +435,7 @@ tsr_status tsr_occupancy_get_counts(const tsr_occupancy *o, tsr_occupancy_counts
         out->visited_priors = o->visits[2];
         out->pruned_leaves = o->pruned;
         out->repaired_leaves = o->repaired;
+        out->certified_leaves = o->certified;
     });
 }
 

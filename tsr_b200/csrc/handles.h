@@ -49,6 +49,7 @@ struct tsr_occupancy {
     uint64_t links = 0;
     uint64_t pruned = 0;             // leaves whose prior query the pruned field skipped
     uint64_t repaired = 0;           // skipped leaves queried after all (bordering a sign change)
+    uint64_t certified = 0;          // skip candidates whose sign the prior bounds proved
 };
 
 struct tsr_mesh {

@@ -196,21 +196,59 @@ __global__ void k_pack_rec(uint32_t nn, const uint32_t *children, const uint32_t
 
 // Pruned field: which leaves need their prior.  Only a reliable leaf
 // (E + S >= confidenceThreshold) uses it, and with E == 0 or S == 0 its sign
-// is fixed without it; of the rest, the pruner lets a leaf skip the query
-// when it is neither near a predicted sign change (PRED_KEEP) nor of
-// uncertain sign (PRED_POS / PRED_NEG clear).
+// is fixed without it (need 0).  A leaf near a predicted sign change
+// (PRED_KEEP), or one whose sign the network is unsure of, is queried
+// (need 1); any other leaf is a candidate for skipping (need 2): its sign is
+// then certified from bounds of its prior (k_certify) or it is queried after
+// all.
+constexpr uint8_t NEED_NONE = 0, NEED_QUERY = 1, NEED_CERTIFY = 2;
+// Levels above the query leaf's depth at which the bounds query stops
+// descending straddling nodes (0: nodes of the leaf's size and smaller).
+#ifndef TSR_PRIOR_BOUND_LEVELS
+#define TSR_PRIOR_BOUND_LEVELS 0
+#endif
+constexpr uint32_t PRIOR_BOUND_LEVELS = TSR_PRIOR_BOUND_LEVELS;
+
 __global__ void k_prior_needed(uint32_t nl, const uint8_t *pred, const double *esum, const double *ssum,
                                double threshold, uint8_t *need) {
     uint32_t l = blockIdx.x * blockDim.x + threadIdx.x;
     if (l >= nl) return;
     const double e = esum[l], s = ssum[l];
     const uint8_t pr = pred[l];
-    bool n = false;
-    if (!((e + s) < threshold)) {
-        if (pr & PRED_KEEP) n = true;
-        else if (e > 0.0 && s > 0.0 && !(pr & (PRED_POS | PRED_NEG))) n = true;
+    uint8_t n = NEED_NONE;
+    if (!((e + s) < threshold) && e > 0.0 && s > 0.0)
+        n = ((pr & PRED_KEEP) || !(pr & (PRED_POS | PRED_NEG))) ? NEED_QUERY : NEED_CERTIFY;
+    else if (!((e + s) < threshold) && (pr & PRED_KEEP))
+        n = NEED_QUERY;
+    need[l] = n;
+}
+
+// The sign of a skip candidate from bounds [lo, hi] of its prior p: the
+// occupancy is positive iff (1 - p) S > p E (Occupancy.cpp:570-587; the
+// common factor 1 / coneCount dropped), which decreases in p.  Positive when
+// it holds at p = hi, negative when it fails at p = lo, each with a relative
+// margin of 1e-9 that covers the rounding of the sums and of the exact
+// formula; otherwise the leaf is queried (need 1).  A certified leaf's sign
+// goes to its PRED_POS / PRED_NEG bits, which the pruned k_finalize uses.
+__global__ void k_certify(uint32_t n, const uint32_t *list, const double *esum, const double *ssum,
+                          const double2 *bounds, uint8_t *pred, uint8_t *need, unsigned long long *certified) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    bool ok = false;
+    if (i < n) {
+        const uint32_t l = list[i];
+        const double e = esum[l], s = ssum[l];
+        const double2 b = bounds[i];
+        const double margin = 1e-9 * (s + e);
+        const bool pos = (1.0 - b.y) * s - b.y * e > margin;
+        const bool neg = (1.0 - b.x) * s - b.x * e < -margin;
+        const uint8_t keep = pred[l] & PRED_KEEP;
+        if (pos) pred[l] = keep | PRED_POS;
+        else if (neg) pred[l] = keep | PRED_NEG;
+        ok = pos || neg;
+        need[l] = ok ? NEED_NONE : NEED_QUERY;
     }
-    need[l] = n ? 1 : 0;
+    const unsigned m = __ballot_sync(0xffffffffu, ok);
+    if ((threadIdx.x & 31) == 0 && m) atomicAdd(certified, (unsigned long long)__popc(m));
 }
 
 __device__ __forceinline__ F3 child_min(F3 pmin, uint32_t ci, float size) {
@@ -531,6 +569,11 @@ __global__ void k_repair_mark(uint32_t nl, const uint32_t *nb_off, const uint32_
     }
 }
 
+__global__ void k_flag_equal(uint32_t n, const uint8_t *v, uint8_t value, uint8_t *flag) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) flag[i] = v[i] == value ? 1 : 0;
+}
+
 __global__ void k_set_needed(uint32_t n, const uint32_t *list, uint8_t *need) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) need[list[i]] = 1;
@@ -649,12 +692,21 @@ __device__ inline bool box_inside_sphere(const D3 &mn, double sz, const D3 &c, d
 // 64-byte line and their FP64 boxes are derived from the parent's corner with
 // the tree build's own recurrence (child_coords, exact), so no node geometry
 // is loaded inside the loop.
+//
+// BOUNDS (the pruned field's sign certificates): a node that straddles the
+// sphere at depth >= the query leaf's depth - coarse_up is not descended;
+// its whole subtree row is added to an undecided pair (eU, sU) instead, so
+// the query ends early with eL <= E <= eL + eU and sL <= S <= sL + sU for
+// the exact sums E, S, and writes bounds[i] = (eL / (eL + sL + sU),
+// (eL + eU) / (eL + eU + sL)) around the prior E / (E + S).
+template <bool BOUNDS>
 __global__ void __launch_bounds__(PT_BLOCK, TSR_PRIOR_BLOCKS) k_priors_x(uint32_t nl, uint32_t nn, const uint32_t *list,
                                                       const uint32_t *leaf_node, const D3 *leaf_min,
                                                       const uint8_t *depth, const D3 *nmin, const uint2 *rec,
                                                       const double2 *psum, double root_size, double rel_radius,
                                                       double *prior, unsigned long long *next_leaf,
-                                                      unsigned long long *visits, int *err) {
+                                                      unsigned long long *visits, int *err, double2 *bounds,
+                                                      uint32_t coarse_up) {
     const unsigned FULL = 0xffffffffu;
     const unsigned lane = threadIdx.x & 31;
     uint64_t st[MAX_TREE_DEPTH];   // children block | mask << 32 | depth << 40
@@ -662,9 +714,9 @@ __global__ void __launch_bounds__(PT_BLOCK, TSR_PRIOR_BLOCKS) k_priors_x(uint32_
     bool have = false, active = false, done = false;
     uint32_t x_c0 = 0, x_d = 0;
     D3 x_min{0.0, 0.0, 0.0};
-    uint32_t l = 0, max_depth = 0;
+    uint32_t l = 0, max_depth = 0, qi = 0, stop_depth = 0;
     D3 center{0.0, 0.0, 0.0};
-    double radius = 0.0, eL = 0.0, sL = 0.0;
+    double radius = 0.0, eL = 0.0, sL = 0.0, eU = 0.0, sU = 0.0;
     float r2f = 0.0f;
     unsigned long long nvis = 0;
     auto add_row = [&](uint32_t n, uint32_t k) {
@@ -685,7 +737,10 @@ __global__ void __launch_bounds__(PT_BLOCK, TSR_PRIOR_BLOCKS) k_priors_x(uint32_
             have = true;
         }
         if (!have && active) {   // query finished
-            prior[l] = eL / (eL + sL);
+            if (BOUNDS)
+                bounds[qi] = make_double2(eL / (eL + sL + sU), (eL + eU) / (eL + eU + sL));
+            else
+                prior[l] = eL / (eL + sL);
             active = false;
         }
         bool need = !have && !done;
@@ -700,9 +755,11 @@ __global__ void __launch_bounds__(PT_BLOCK, TSR_PRIOR_BLOCKS) k_priors_x(uint32_
                 if (i >= nl) {
                     done = true;
                 } else {
+                    qi = (uint32_t)i;
                     l = list ? list[i] : (uint32_t)i;
                     uint32_t node = leaf_node[l];
                     uint32_t ld = depth[node];
+                    stop_depth = ld > coarse_up + 1 ? ld - coarse_up : 1;
                     double size = size_at(root_size, ld);
                     D3 mn = leaf_min[l];
                     double half = dmul(0.5, size);
@@ -710,7 +767,7 @@ __global__ void __launch_bounds__(PT_BLOCK, TSR_PRIOR_BLOCKS) k_priors_x(uint32_
                     radius = dmul(size, rel_radius);
                     r2f = (float)dmul(radius, radius);
                     max_depth = ld + MAX_DEPTH_DIFFERENCE;
-                    eL = sL = 0.0;
+                    eL = sL = eU = sU = 0.0;
                     active = true;
                     // the root (SphereNodeStatesChecker on node 0)
                     uint2 r0 = __ldg(&rec[REC_OFFSET]);
@@ -764,6 +821,7 @@ __global__ void __launch_bounds__(PT_BLOCK, TSR_PRIOR_BLOCKS) k_priors_x(uint32_
             const float ex = 4e-7f * (fabsf(rx0) + 2.0f * csf), ey = 4e-7f * (fabsf(ry0) + 2.0f * csf),
                         ez = 4e-7f * (fabsf(rz0) + 2.0f * csf);
             double2 v[8];
+            uint32_t umask = 0;
 #pragma unroll
             for (int ci = 0; ci < 8; ++ci) {
                 const bool flagged = (ry[ci] & REC_FLAG) != 0;
@@ -791,14 +849,23 @@ __global__ void __launch_bounds__(PT_BLOCK, TSR_PRIOR_BLOCKS) k_priors_x(uint32_
                     inside = can_add && box_inside_sphere(bmn, cs, center, radius);
                 }
                 meets = meets && flagged;
-                const size_t row = (size_t)(inside ? max_depth - d : 0u) * nn + x_c0 + ci;
-                v[ci] = (meets && (inside || leaf)) ? __ldg(&psum[row]) : make_double2(0.0, 0.0);
-                if (meets && !inside && !leaf && can_descend) mask |= 1u << ci;
+                // BOUNDS: a straddling node at or below the stop depth is undecided
+                // (max_depth - d <= 3 + coarse_up < PK there)
+                const bool unc = BOUNDS && meets && !inside && !leaf && d >= stop_depth;
+                const size_t row = (size_t)((inside || unc) ? max_depth - d : 0u) * nn + x_c0 + ci;
+                v[ci] = (meets && (inside || leaf || unc)) ? __ldg(&psum[row]) : make_double2(0.0, 0.0);
+                if (unc) umask |= 1u << ci;
+                if (meets && !inside && !leaf && can_descend && !unc) mask |= 1u << ci;
             }
 #pragma unroll
             for (int ci = 0; ci < 8; ++ci) {
-                eL += v[ci].x;
-                sL += v[ci].y;
+                if (BOUNDS && ((umask >> ci) & 1u)) {
+                    eU += v[ci].x;
+                    sU += v[ci].y;
+                } else {
+                    eL += v[ci].x;
+                    sL += v[ci].y;
+                }
             }
         }
         if (mask) {
@@ -934,7 +1001,7 @@ void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_
         TSR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         TSR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cone_x<EMPTINESS>, PT_BLOCK, 0));
         x_grid = (unsigned)(sms * (per_sm > 0 ? per_sm : 1));
-        TSR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_priors_x, PT_BLOCK, 0));
+        TSR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_priors_x<false>, PT_BLOCK, 0));
         prior_grid = (unsigned)(sms * (per_sm > 0 ? per_sm : 1));
     }
     if (nl > REC_NOLEAF) fail(TSR_ERR_OVERFLOW_U32, "leaf count must stay below 2^31 - 1 for the traversal records");
@@ -1017,27 +1084,48 @@ void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_
         // the queried leaves: all of them, or the selected ones of a pruned field
         DBuf<uint32_t> list;
         uint32_t nq = nl;
-        if (pred) {
-            DBuf<uint32_t> ids(nl, st), nsel(1, st);
-            list.alloc(nl, st);
-            k_iota<<<grid_for(nl, BLK), BLK, 0, st>>>(nl, ids.p); ::tsr::note_launch();
-            size_t tmp = 0;
-            TSR_CUDA(cub::DeviceSelect::Flagged(nullptr, tmp, ids.p, need.p, list.p, nsel.p, (int)nl, st));
-            DBuf<uint8_t> tb(tmp, st);
-            TSR_CUDA(cub::DeviceSelect::Flagged(tb.p, tmp, ids.p, need.p, list.p, nsel.p, (int)nl, st));
-            nq = read_scalar(nsel.p, st);
-            o.pruned = nl - nq;
-        }
         psum.alloc((size_t)nn * PK, st);
         for (int d = (int)t.level_start.size() - 2; d >= 0; --d) {
             uint32_t lo = t.level_start[d], hi = t.level_start[d + 1];
             k_prior_sums<<<grid_for(hi - lo, BLK), BLK, 0, st>>>(lo, hi, nn, t.level_order.p, t.children.p,
                                                                 t.node_to_leaf.p, o.states.p, elen, slen, psum.p); ::tsr::note_launch();
         }
+        if (pred) {
+            DBuf<uint32_t> ids(nl, st), nsel(1, st), clist(nl, st);
+            DBuf<uint8_t> cflag(nl, st);
+            DBuf<unsigned long long> ncert(1, st);
+            ncert.zero();
+            list.alloc(nl, st);
+            k_iota<<<grid_for(nl, BLK), BLK, 0, st>>>(nl, ids.p); ::tsr::note_launch();
+            size_t tmp = 0;
+            TSR_CUDA(cub::DeviceSelect::Flagged(nullptr, tmp, ids.p, need.p, list.p, nsel.p, (int)nl, st));
+            DBuf<uint8_t> tb(tmp, st);
+            // skip candidates: certify their signs from bounds of their priors
+            k_flag_equal<<<grid_for(nl, BLK), BLK, 0, st>>>(nl, need.p, NEED_CERTIFY, cflag.p); ::tsr::note_launch();
+            TSR_CUDA(cub::DeviceSelect::Flagged(tb.p, tmp, ids.p, cflag.p, clist.p, nsel.p, (int)nl, st));
+            const uint32_t nc = read_scalar(nsel.p, st);
+            if (nc) {
+                DBuf<double2> bnd(nc, st);
+                next_link.zero();
+                k_priors_x<true><<<prior_grid, PT_BLOCK, 0, st>>>(nc, nn, clist.p, t.leaf_node.p, t.leaf_min.p,
+                                                                  t.depth.p, t.nmin.p, recs.p, psum.p, t.root_size,
+                                                                  p.relative_radius_for_priors, nullptr, next_link.p,
+                                                                  accepted.p + 4, err.p, bnd.p, PRIOR_BOUND_LEVELS);
+                ::tsr::note_launch();
+                k_certify<<<grid_for(nc, BLK), BLK, 0, st>>>(nc, clist.p, esum, ssum, bnd.p, pred_buf.p, need.p,
+                                                            ncert.p); ::tsr::note_launch();
+                o.certified = read_scalar(ncert.p, st);
+            }
+            // every leaf still needing its prior (need 1) is queried
+            TSR_CUDA(cub::DeviceSelect::Flagged(tb.p, tmp, ids.p, need.p, list.p, nsel.p, (int)nl, st));
+            nq = read_scalar(nsel.p, st);
+            o.pruned = nl - nq;
+        }
         next_link.zero();
-        k_priors_x<<<prior_grid, PT_BLOCK, 0, st>>>(nq, nn, list.p, t.leaf_node.p, t.leaf_min.p, t.depth.p, t.nmin.p, recs.p,
-                                                   psum.p, t.root_size, p.relative_radius_for_priors, o.prior.p,
-                                                   next_link.p, accepted.p + 4, err.p);
+        k_priors_x<false><<<prior_grid, PT_BLOCK, 0, st>>>(nq, nn, list.p, t.leaf_node.p, t.leaf_min.p, t.depth.p,
+                                                          t.nmin.p, recs.p, psum.p, t.root_size,
+                                                          p.relative_radius_for_priors, o.prior.p, next_link.p,
+                                                          accepted.p + 4, err.p, nullptr, 0);
         ::tsr::note_launch();
     }
     o.stage_ms[3] = timer.lap();
@@ -1070,10 +1158,10 @@ void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_
             if (nf == 0) break;
             k_set_needed<<<grid_for(nf, BLK), BLK, 0, st>>>(nf, flist.p, need.p); ::tsr::note_launch();
             next_link.zero();
-            k_priors_x<<<prior_grid, PT_BLOCK, 0, st>>>(nf, nn, flist.p, t.leaf_node.p, t.leaf_min.p, t.depth.p,
-                                                       t.nmin.p, recs.p, psum.p, t.root_size,
-                                                       p.relative_radius_for_priors, o.prior.p, next_link.p,
-                                                       accepted.p + 4, err.p); ::tsr::note_launch();
+            k_priors_x<false><<<prior_grid, PT_BLOCK, 0, st>>>(nf, nn, flist.p, t.leaf_node.p, t.leaf_min.p,
+                                                              t.depth.p, t.nmin.p, recs.p, psum.p, t.root_size,
+                                                              p.relative_radius_for_priors, o.prior.p, next_link.p,
+                                                              accepted.p + 4, err.p, nullptr, 0); ::tsr::note_launch();
             k_finalize<<<grid_for(nl, BLK), BLK, 0, st>>>(nl, esum, ssum, elen, slen, o.prior.p, o.cone_count,
                                                          p.confidence_threshold, pred, need.p, o.e_sum.p, o.s_sum.p,
                                                          o.e_len.p, o.s_len.p, o.occ.p); ::tsr::note_launch();

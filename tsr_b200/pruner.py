@@ -185,6 +185,30 @@ def vertex_hausdorff(a, b):
     return float(max(cKDTree(b).query(a)[0].max(), cKDTree(a).query(b)[0].max()))
 
 
+def emptiness_needed_fraction(tree, plain, pruned, rel_radius=25.0):
+    """How much of the EMPTINESS pass a cone-pass pruner could skip without
+    changing the pruned field's exact values: the share of the leaves that
+    received EMPTINESS kernels (and of their kernel sum) lying inside the
+    prior sphere (rel_radius leaf sizes) of some leaf whose prior the pruned
+    field queries.  Those leaves' EMPTINESS lengths enter a queried prior, so
+    their cone contributions are needed exactly."""
+    from scipy.spatial import cKDTree
+    sc = tree.getLeaves().scopes
+    centers = sc[:, :3] + 0.5 * sc[:, 3:4]
+    queried = np.isfinite(pruned.getPriorForEmptiness())
+    e = plain.field("emptiness_sum")
+    got = e > 0
+    if not queried.any() or not got.any():
+        return {"leaves": 0.0, "kernel_sum": 0.0}
+    needed = np.zeros(got.sum(), bool)
+    pts = centers[got]
+    qs, qc = sc[queried, 3], centers[queried]
+    for size in np.unique(qs):   # one radius per leaf size
+        kd = cKDTree(qc[qs == size])
+        needed |= kd.query_ball_point(pts, rel_radius * size, return_length=True) > 0
+    return {"leaves": float(needed.mean()), "kernel_sum": float(e[got][needed].sum() / e[got].sum())}
+
+
 def judge(tree, cams, pruner, params=None, stream=None):
     """The plain method judges the pruned field: both fields and meshes on
     the same tree, with the pruned field's error and work savings."""
@@ -198,6 +222,7 @@ def judge(tree, cams, pruner, params=None, stream=None):
         "leaves": int(op.shape[0]),
         "pruned_leaves": pruned.counts["pruned_leaves"],
         "repaired_leaves": pruned.counts["repaired_leaves"],
+        "certified_leaves": pruned.counts["certified_leaves"],
         "sign_agreement": float(np.mean((op > 0) == (oq > 0))),
         "case_agreement": float(np.mean(mesh_plain.cases == mesh_pruned.cases)),
         "triangles": [int(mesh_plain.triangles.shape[0]), int(mesh_pruned.triangles.shape[0])],
