@@ -136,6 +136,8 @@ typedef struct {
                                           or above 1 - this (0 < sign_threshold < 0.5) */
     float band_threshold;              /* a leaf counts as near a sign change when P(band) >= this */
     uint32_t dilation;                 /* rings of face neighbours added around those leaves */
+    uint32_t bound_levels;             /* a skip candidate's sign is certified by a bounds query that
+                                          stops at nodes this many levels above the leaf (0 .. 4) */
 } tsr_pruner;
 
 typedef struct tsr_tree tsr_tree;
@@ -336,8 +338,9 @@ TSR_API tsr_status tsr_mlp_infer_bf16(const float *x, uint32_t n, const float *p
  * a sign change (or within `dilation` rings of face neighbours of one), whose
  * sign it is not sure of, or whose sign cannot be certified; E == 0 or
  * S == 0 fixes the sign without a prior.  Every other reliable leaf gets a
- * cheaper bounds query (the prior's sphere query stopped at nodes of the
- * leaf's size, their subtrees counted as undecided), and is skipped only when
+ * cheaper bounds query (the prior's sphere query stopped at nodes
+ * `bound_levels` levels above the leaf's depth, their subtrees counted as
+ * undecided), and is skipped only when
  * the bounds prove its sign ((1 - p) S > p E for every p in them, or for
  * none); it then takes that sign, with the value 0.5 (S - E) / coneCount
  * when positive, and its prior reads NaN.  Skipped leaves that border a leaf

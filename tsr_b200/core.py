@@ -77,7 +77,7 @@ class tsr_mesh_post_counts(ctypes.Structure):
 class tsr_pruner(ctypes.Structure):
     _fields_ = [("weights", _P), ("feature_mean", ctypes.c_float * MLP_FEATURES),
                 ("feature_inv_std", ctypes.c_float * MLP_FEATURES), ("sign_threshold", ctypes.c_float),
-                ("band_threshold", ctypes.c_float), ("dilation", _U32)]
+                ("band_threshold", ctypes.c_float), ("dilation", _U32), ("bound_levels", _U32)]
 
 
 lib = ctypes.CDLL(str(_LIB_PATH))
@@ -702,7 +702,7 @@ class Pruner:
     (W1[10][64], b1, W2[64][64], b2, W3[64][2], b3); features are normalized
     as (f - mean) * inv_std."""
 
-    def __init__(self, weights, mean, inv_std, sign_threshold, band_threshold, dilation=1):
+    def __init__(self, weights, mean, inv_std, sign_threshold, band_threshold, dilation=1, bound_levels=2):
         self.weights = np.ascontiguousarray(weights, np.float32).reshape(-1)
         if self.weights.shape[0] != MLP_PARAMS:
             raise ValueError("expected %d weights" % MLP_PARAMS)
@@ -711,13 +711,14 @@ class Pruner:
         self.sign_threshold = float(sign_threshold)
         self.band_threshold = float(band_threshold)
         self.dilation = int(dilation)
+        self.bound_levels = int(bound_levels)
 
     @classmethod
     def load(cls, path=None):
         path = Path(path) if path else Path(__file__).resolve().parent / "pruner_weights.npz"
         z = np.load(path)
         self = cls(z["weights"], z["mean"], z["inv_std"], float(z["sign_threshold"]), float(z["band_threshold"]),
-                   int(z["dilation"]))
+                   int(z["dilation"]), int(z["bound_levels"]) if "bound_levels" in z.files else 2)
         self.meta = json.loads(str(z["meta"])) if "meta" in z.files else {}
         self.path = str(path)
         return self
@@ -735,7 +736,7 @@ class Pruner:
     def save(self, path, **extra):
         np.savez(path, weights=self.weights, mean=self.mean, inv_std=self.inv_std,
                  sign_threshold=np.float32(self.sign_threshold), band_threshold=np.float32(self.band_threshold),
-                 dilation=np.int32(self.dilation), **extra)
+                 dilation=np.int32(self.dilation), bound_levels=np.int32(self.bound_levels), **extra)
 
     def view(self):
         v = tsr_pruner()
@@ -746,6 +747,7 @@ class Pruner:
         v.sign_threshold = self.sign_threshold
         v.band_threshold = self.band_threshold
         v.dilation = self.dilation
+        v.bound_levels = self.bound_levels
         self._keep = self.weights   # the C side reads the weights during the call
         return v
 

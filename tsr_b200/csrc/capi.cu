@@ -329,6 +329,7 @@ tsr_status tsr_occupancy_compute_pruned(const tsr_tree *tree, const tsr_cameras_
             !(pruner->band_threshold > 0.0f && pruner->band_threshold < 1.0f))
             fail(TSR_ERR_INVALID_ARG, "pruner thresholds: sign in (0, 0.5), band in (0, 1)");
         if (pruner->dilation > 64) fail(TSR_ERR_INVALID_ARG, "pruner dilation above 64 rings");
+        if (pruner->bound_levels > 4) fail(TSR_ERR_INVALID_ARG, "pruner bound_levels above 4");
         if (cameras->count && !cameras->positions) fail(TSR_ERR_INVALID_ARG, "null camera positions");
         if (tree->n_leaves == 0) fail(TSR_ERR_STATE, "tree has no leaves");
         tsr_params p = tree->params;

@@ -202,12 +202,7 @@ __global__ void k_pack_rec(uint32_t nn, const uint32_t *children, const uint32_t
 // then certified from bounds of its prior (k_certify) or it is queried after
 // all.
 constexpr uint8_t NEED_NONE = 0, NEED_QUERY = 1, NEED_CERTIFY = 2;
-// Levels above the query leaf's depth at which the bounds query stops
-// descending straddling nodes (0: nodes of the leaf's size and smaller).
-#ifndef TSR_PRIOR_BOUND_LEVELS
-#define TSR_PRIOR_BOUND_LEVELS 0
-#endif
-constexpr uint32_t PRIOR_BOUND_LEVELS = TSR_PRIOR_BOUND_LEVELS;
+
 
 __global__ void k_prior_needed(uint32_t nl, const uint8_t *pred, const double *esum, const double *ssum,
                                double threshold, uint8_t *need) {
@@ -1110,7 +1105,7 @@ void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_
                 k_priors_x<true><<<prior_grid, PT_BLOCK, 0, st>>>(nc, nn, clist.p, t.leaf_node.p, t.leaf_min.p,
                                                                   t.depth.p, t.nmin.p, recs.p, psum.p, t.root_size,
                                                                   p.relative_radius_for_priors, nullptr, next_link.p,
-                                                                  accepted.p + 4, err.p, bnd.p, PRIOR_BOUND_LEVELS);
+                                                                  accepted.p + 4, err.p, bnd.p, pruner->bound_levels);
                 ::tsr::note_launch();
                 k_certify<<<grid_for(nc, BLK), BLK, 0, st>>>(nc, clist.p, esum, ssum, bnd.p, pred_buf.p, need.p,
                                                             ncert.p); ::tsr::note_launch();
