@@ -241,6 +241,9 @@ def main():
     ap.add_argument("--samples-min", type=int, default=2_000_000)
     ap.add_argument("--samples-max", type=int, default=4_000_000)
     ap.add_argument("--host-scenes", action="store_true", help="render the scenes with numpy on the host")
+    ap.add_argument("--width", type=int, default=2200, help="camera image width of the training scenes")
+    ap.add_argument("--height", type=int, default=1650)
+    ap.add_argument("--f", type=float, default=1650.0, help="focal length in pixels")
     ap.add_argument("--epochs", type=int, default=4)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--miss", type=float, default=1e-3)
@@ -258,7 +261,7 @@ def main():
         if a.host_scenes:
             return lambda: scenes.random_csg_scene(seed=1 + i, n_target=n)
         noisy = i % 3 == 2 and i != a.scenes - 1
-        return lambda: scenes.random_csg_scene_device(1 + i, n, 1600, 1200, 1200.0,
+        return lambda: scenes.random_csg_scene_device(1 + i, n, a.width, a.height, a.f,
                                                       outlier_frac=0.05 if noisy else 0.0,
                                                       conf_range=(0.2, 1.0) if noisy else (1.0, 1.0))
 
