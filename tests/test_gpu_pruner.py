@@ -15,6 +15,7 @@ pytestmark = pytest.mark.gpu
 MIN_CASE_AGREEMENT = 1.0          # DMC case codes equal to the plain field's
 MAX_HAUSDORFF_LEAVES = 0.0        # vertex Hausdorff distance, in finest leaf sizes
 MIN_PRIOR_WORK_SAVED = 0.15       # fraction of prior-query node visits removed
+MIN_EMPTINESS_NEEDED = 0.9        # share of the EMPTINESS kernel sum inside a queried leaf's prior sphere
 
 
 @pytest.fixture(scope="module")
@@ -69,3 +70,19 @@ def test_pruned_field_is_exact_on_a_cluttered_scene():
     assert j["case_agreement"] == 1.0, j
     assert j["vertex_hausdorff"] == 0.0, j
     assert j["pruned_leaves"] > 0, j
+
+
+def test_emptiness_pass_is_needed_by_the_queried_priors(heldout):
+    """Why the pruned field keeps the EMPTINESS pass exact: almost every leaf
+    that receives EMPTINESS kernels lies inside the prior sphere (25 leaf
+    sizes) of a leaf whose prior the pruned field still queries, so its cone
+    lengths enter an exact prior -- skipping its cone contributions would
+    change a queried leaf's value.  Measured share logged; asserted high."""
+    from fieldcheck import log
+    from tsr_b200 import core, pruner
+    tree, cams = heldout
+    plain = core.Occupancy(tree, cams)
+    pruned = core.Occupancy(tree, cams, pruner=core.Pruner.load())
+    f = pruner.emptiness_needed_fraction(tree, plain, pruned)
+    log({"test": "emptiness_needed", **f})
+    assert f["kernel_sum"] >= MIN_EMPTINESS_NEEDED, f

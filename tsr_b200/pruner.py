@@ -16,8 +16,11 @@ and whose sign it is sure of.
 
     python -m tsr_b200.pruner --scenes 50 --out tsr_b200/pruner_weights.npz
 
-The committed ``pruner_weights.npz`` was produced by that command (its
-``meta`` entry records the arguments and the training statistics).
+trains on 49 seeded random CSG scenes of 2-4M samples (every third with
+outliers and varying confidences), rendered on the GPU, and picks the
+thresholds on the 50th.  The committed ``pruner_weights.npz`` was produced by
+that command (its ``meta`` entry records the arguments and the training
+statistics).
 """
 from __future__ import annotations
 
@@ -241,13 +244,14 @@ def main():
     ap.add_argument("--samples-min", type=int, default=2_000_000)
     ap.add_argument("--samples-max", type=int, default=4_000_000)
     ap.add_argument("--host-scenes", action="store_true", help="render the scenes with numpy on the host")
-    ap.add_argument("--width", type=int, default=2200, help="camera image width of the training scenes")
-    ap.add_argument("--height", type=int, default=1650)
-    ap.add_argument("--f", type=float, default=1650.0, help="focal length in pixels")
+    ap.add_argument("--width", type=int, default=800, help="camera image width of the training scenes")
+    ap.add_argument("--height", type=int, default=600)
+    ap.add_argument("--f", type=float, default=600.0, help="focal length in pixels")
     ap.add_argument("--epochs", type=int, default=4)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--miss", type=float, default=1e-3)
-    ap.add_argument("--dilation", type=int, default=1)
+    ap.add_argument("--dilation", type=int, default=0)
+    ap.add_argument("--bound-levels", type=int, default=3)
     ap.add_argument("--out", default="pruner_weights.npz")
     a = ap.parse_args()
     from . import scenes
@@ -267,6 +271,7 @@ def main():
 
     pruner, stats = fit([maker(i, n) for i, n in enumerate(sizes)], epochs=a.epochs, seed=a.seed, miss=a.miss,
                         dilation=a.dilation)
+    pruner.bound_levels = a.bound_levels
     stats["args"] = vars(a)
     stats["samples_per_scene"] = sizes
     print(json.dumps(stats), flush=True)
