@@ -517,7 +517,7 @@ def our_arm(args):
                      "share_of_step": stages[dom] / total_ms if total_ms else None, "traffic": traffic,
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per unit on csg1m, "
                                        "scaled to this run's units"},
-        # the survey's secondary figures: the traversals' work rates (what bounds them, not HBM)
+        # secondary figures: the traversals' work rates (what bounds them, not HBM)
         "secondary": {
             "node_tests_per_s": {"sampleness": oc.visited_sampleness / (stages["occ.sampleness"] / 1e3),
                                  "emptiness": oc.visited_emptiness / (stages["occ.emptiness"] / 1e3),

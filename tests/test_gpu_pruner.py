@@ -14,7 +14,7 @@ pytestmark = pytest.mark.gpu
 # field's, case codes and vertices alike.
 MIN_CASE_AGREEMENT = 1.0          # DMC case codes equal to the plain field's
 MAX_HAUSDORFF_LEAVES = 0.0        # vertex Hausdorff distance, in finest leaf sizes
-MIN_PRIOR_WORK_SAVED = 0.15       # fraction of prior-query node visits removed
+MIN_PRIOR_WORK_SAVED = 0.4        # fraction of prior-query node visits removed
 MIN_EMPTINESS_NEEDED = 0.9        # share of the EMPTINESS kernel sum inside a queried leaf's prior sphere
 
 
