@@ -343,11 +343,18 @@ __device__ inline uint32_t descent_leaf_v(const NV &v, const Root &root, uint32_
 // Round evaluation: status 1 = reliable (witness), 2 = writer.  Also counts
 // each side's dependency pairs (1 for a witness; the rejected leaves plus the
 // descent leaf for a writer).
+// split_sides: the keys are both sides of consecutive samples in turn (the
+// first round); threads then take all positive sides first and all negative
+// sides after them, so the lanes of a warp search in the same direction
+// (the two sides' searches differ, and a warp waits for its longest one).
+// Results go to each side's own slot either way.
 __global__ void k_sampling_eval(uint32_t m, const uint32_t *keys, NV v, Root root, const D3 *pos, const D3 *nrm,
                                 const double *scale, double h_svo, uint8_t *status, uint32_t *witness,
-                                uint32_t *dleaf, uint32_t *cnt, double margin, int *err) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= m) return;
+                                uint32_t *dleaf, uint32_t *cnt, double margin, int *err, int split_sides) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= m) return;
+    const uint32_t half = (m + 1) / 2;
+    const uint32_t i = split_sides ? (t < half ? 2 * t : 2 * (t - half) + 1) : t;
     uint32_t key = keys[i];
     SampleRef q = sample_side(key, pos, nrm, scale, h_svo);
     int e = 0;
@@ -1188,7 +1195,8 @@ void build_tree(tsr_tree &t, const tsr_samples_view &sv, bool on_device) {
             TSR_CUDA(cudaMemsetAsync(scnt.p + m, 0, 4, st));
             TSR_CUDA(cudaEventRecord(e0, st));
             k_sampling_eval<<<grid_for(m, 128), 128, 0, st>>>(m, keys.p, v, root, pos.p, nrm.p, scale.p, h_svo,
-                                                             status.p, witness.p, dleaf.p, scnt.p, margin, derr.p);
+                                                             status.p, witness.p, dleaf.p, scnt.p, margin, derr.p,
+                                                             rounds == 1 ? 1 : 0);
             ::tsr::note_launch();
             TSR_CUDA(cudaEventRecord(e1, st));
             // dependency index (leaf -> sides) and the writer list
