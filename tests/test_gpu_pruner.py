@@ -86,3 +86,23 @@ def test_emptiness_pass_is_needed_by_the_queried_priors(heldout):
     f = pruner.emptiness_needed_fraction(tree, plain, pruned)
     log({"test": "emptiness_needed", **f})
     assert f["kernel_sum"] >= MIN_EMPTINESS_NEEDED, f
+
+
+def test_network_against_certifying_every_leaf(heldout):
+    """What the network adds over the sign certificates alone: the same
+    pruned field with the network's band prediction switched off (every
+    reliable leaf gets a bounds query).  Both meshes are the plain field's;
+    the prior-query work of both is logged beside the plain field's."""
+    from fieldcheck import log
+    from tsr_b200 import core, pruner
+    tree, cams = heldout
+    net = core.Pruner.load()
+    alone = core.Pruner.load()
+    alone.band_threshold = 0.999999
+    alone.sign_threshold = 0.4999
+    jn = pruner.judge(tree, cams, net)
+    ja = pruner.judge(tree, cams, alone)
+    log({"test": "network_vs_certify_all", "network": jn["visited"]["visited_priors"],
+         "certify_all": ja["visited"]["visited_priors"], "pruned": [jn["pruned_leaves"], ja["pruned_leaves"]]})
+    for j in (jn, ja):
+        assert j["case_agreement"] == 1.0 and j["vertex_hausdorff"] == 0.0, j

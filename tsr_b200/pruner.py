@@ -252,6 +252,9 @@ def main():
     ap.add_argument("--miss", type=float, default=1e-3)
     ap.add_argument("--dilation", type=int, default=0)
     ap.add_argument("--bound-levels", type=int, default=3)
+    ap.add_argument("--band-deploy", type=float, default=0.99,
+                    help="band threshold stored for use (the chosen miss rate's threshold stays in meta); "
+                         "exactness does not depend on it, speed does")
     ap.add_argument("--out", default="pruner_weights.npz")
     a = ap.parse_args()
     from . import scenes
@@ -272,6 +275,9 @@ def main():
     pruner, stats = fit([maker(i, n) for i, n in enumerate(sizes)], epochs=a.epochs, seed=a.seed, miss=a.miss,
                         dilation=a.dilation)
     pruner.bound_levels = a.bound_levels
+    stats["trained_band_threshold"] = pruner.band_threshold
+    if a.band_deploy:
+        pruner.band_threshold = max(pruner.band_threshold, a.band_deploy)
     stats["args"] = vars(a)
     stats["samples_per_scene"] = sizes
     print(json.dumps(stats), flush=True)
