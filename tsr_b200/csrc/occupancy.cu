@@ -815,6 +815,11 @@ __global__ void __launch_bounds__(PT_BLOCK, TSR_PRIOR_BLOCKS) k_priors_x(uint32_
                         rz0 = (float)dsub(x_min.z, center.z);
             const float ex = 4e-7f * (fabsf(rx0) + 2.0f * csf), ey = 4e-7f * (fabsf(ry0) + 2.0f * csf),
                         ez = 4e-7f * (fabsf(rz0) + 2.0f * csf);
+            // Every child reads row krow: an added subtree needs row
+            // max_depth - d (< PK wherever one is added), and a leaf's rows
+            // are all equal, so the eight children's pairs come from one
+            // 128-byte line.
+            const uint32_t krow = max_depth - d < (uint32_t)PK ? max_depth - d : (uint32_t)PK - 1u;
             double2 v[8];
             uint32_t umask = 0;
 #pragma unroll
@@ -847,7 +852,7 @@ __global__ void __launch_bounds__(PT_BLOCK, TSR_PRIOR_BLOCKS) k_priors_x(uint32_
                 // BOUNDS: a straddling node at or below the stop depth is undecided
                 // (max_depth - d <= 3 + coarse_up < PK there)
                 const bool unc = BOUNDS && meets && !inside && !leaf && d >= stop_depth;
-                const size_t row = (size_t)((inside || unc) ? max_depth - d : 0u) * nn + x_c0 + ci;
+                const size_t row = (size_t)krow * nn + x_c0 + ci;
                 v[ci] = (meets && (inside || leaf || unc)) ? __ldg(&psum[row]) : make_double2(0.0, 0.0);
                 if (unc) umask |= 1u << ci;
                 if (meets && !inside && !leaf && can_descend && !unc) mask |= 1u << ci;
