@@ -51,5 +51,6 @@ def field_stats(ref_fields, gpu, leaves):
     out["sign_flips"] = [int(x) for x in flips[:50]]
     out["sign_flip_count"] = int(flips.size)
     out["leaves"] = int(leaves)
-    out["cone_count_rel"] = abs(gpu.field("cone_count") - float(ref_fields["cone_count"])) / float(ref_fields["cone_count"])
+    cc = float(ref_fields["cone_count"])
+    out["cone_count_rel"] = abs(gpu.field("cone_count") - cc) / (abs(cc) if cc != 0.0 else 1.0)
     return out

@@ -8,13 +8,14 @@ reference computes for them: the node arrays, the sample permutation, leaf
 scopes, node->leaf links, the neighbour CSR, dual cells, the occupancy field
 (kernel sums, cone lengths, priors, node states, cone count, occupancy of
 every leaf) and the raw DMC mesh.  Scenes: the two golden scenes of
-make_golden.py, a K = 3 capture with invalid and repeated camera links, and a
-small cluttered capture (outliers, confidences in [0.2, 1]).
+make_golden.py, a K = 3 capture with invalid and repeated camera links, a
+small cluttered capture (outliers, confidences in [0.2, 1]) and the
+degenerate inputs of edge_scenes() (ref_edge_*).
 ref_update_csg_3k.npz holds the incremental update of the CSG fixture's
 field: Occupancy::eraseSamples of 10 % of the samples (tree-order indices,
 seed 4), then Occupancy::addSamples of the same samples.
 
-Usage: python tests/golden/make_ref_golden.py   (needs the reference sources)
+Usage: python tests/golden/make_ref_golden.py [fixture names]   (needs the reference sources)
 """
 import sys
 from pathlib import Path
@@ -45,17 +46,47 @@ def k3_scene():
     return scenes.Scene(sc.pos, sc.nrm, sc.scale, sc.conf, np.ascontiguousarray(links), sc.cams, "sphere_k3")
 
 
+def edge_scenes():
+    """Degenerate inputs: one sample, two samples, every sample three times
+    at the same position, a flat patch (zero extent along z) seen by two
+    cameras, and samples whose every link is invalid (no cones at all)."""
+    base = scenes.sphere_scene(stride=16)
+
+    def sub(idx, name, links=None):
+        return scenes.Scene(base.pos[idx], base.nrm[idx], base.scale[idx], base.conf[idx],
+                            np.ascontiguousarray(base.links[idx] if links is None else links, np.uint32), base.cams,
+                            name)
+
+    rng = np.random.default_rng(1)
+    xy = rng.uniform(-1.0, 1.0, (3000, 2))
+    plane = scenes.Scene(np.c_[xy, np.zeros(3000)], np.tile([0.0, 0.0, 1.0], (3000, 1)), np.full(3000, 0.02),
+                         np.ones(3000), (np.arange(3000, dtype=np.uint32) % 2)[:, None].copy(),
+                         np.array([[0.0, 0.0, 3.0], [1.0, 1.0, 2.0]]), "plane")
+    every = np.arange(0, base.n, 8)
+    return {
+        "ref_edge_single": sub(np.arange(1), "single"),
+        "ref_edge_two": sub(np.arange(2), "two"),
+        "ref_edge_duplicates": sub(np.repeat(np.arange(200), 3), "duplicates"),
+        "ref_edge_plane": plane,
+        "ref_edge_no_links": sub(every, "no_links", np.full((every.shape[0], 1), INVALID, np.uint32)),
+    }
+
+
 def fixture_scenes():
     return {
         "ref_sphere_small": scenes.sphere_scene(stride=6, width=160, height=120, f=125.0),
         "ref_csg_3k": scenes.csg_scene(seed=3, n_target=3000, width=160, height=120, f=125.0, n_cams=12),
         "ref_sphere_k3": k3_scene(),
         "ref_cluttered_2k": scenes.cluttered_scene(seed=2, n_target=2000),
+        **edge_scenes(),
     }
 
 
-def main():
+def main(names=None):
+    """All fixtures, or only those named on the command line."""
     for name, sc in fixture_scenes().items():
+        if names and name not in names:
+            continue
         r = refpy.run(sc, threads=1)
         out = {k: v for k, v in r.items() if k != "fields" and not k.startswith("samples_")}
         out.update({"field_" + k: np.asarray(v) for k, v in r["fields"].items()})
@@ -64,7 +95,8 @@ def main():
         np.savez_compressed(GOLDEN / (name + ".npz"), **inputs, **out)
         print(name, sc.n, "samples, K =", sc.k, ",", out["children"].shape[0], "nodes,", out["tris"].shape[0],
               "triangles")
-    update_fixture()
+    if not names or "ref_update_csg_3k" in names:
+        update_fixture()
 
 
 def update_fixture():
@@ -83,4 +115,4 @@ def update_fixture():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])
