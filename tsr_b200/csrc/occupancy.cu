@@ -574,6 +574,16 @@ __global__ void k_set_needed(uint32_t n, const uint32_t *list, uint8_t *need) {
     if (i < n) need[list[i]] = 1;
 }
 
+// Depth of every listed leaf (list == null: leaves 0 .. n-1) as a sort key.
+__global__ void k_leaf_depth_keys(uint32_t n, const uint32_t *list, const uint32_t *leaf_node, const uint8_t *depth,
+                                  uint32_t *keys, uint32_t *vals) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t l = list ? list[i] : i;
+    keys[i] = depth[leaf_node[l]];
+    vals[i] = l;
+}
+
 __global__ void k_iota(uint32_t n, uint32_t *out) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) out[i] = i;
@@ -944,6 +954,25 @@ struct Timer {
     ~Timer() { cudaEventDestroy(a); cudaEventDestroy(b); }
 };
 
+// Prior queries in order of leaf depth, coarsest first, tree order within a
+// depth (a stable radix sort of 6-bit keys).  A coarse leaf's sphere is wide
+// and its query long; taking those first keeps the persistent lanes from
+// ending on a tail of long queries, and a warp's lanes share one radius.
+static_assert(MAX_TREE_DEPTH <= 64, "depth keys are 6 bits");
+DBuf<uint32_t> depth_ordered(uint32_t n, const uint32_t *list, const uint32_t *leaf_node, const uint8_t *depth,
+                             cudaStream_t st) {
+    DBuf<uint32_t> out(n, st);
+    if (n == 0) return out;
+    DBuf<uint32_t> k1(n, st), k2(n, st), v1(n, st);
+    k_leaf_depth_keys<<<grid_for(n, BLK), BLK, 0, st>>>(n, list, leaf_node, depth, k1.p, v1.p);
+    ::tsr::note_launch();
+    size_t tmp = 0;
+    TSR_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, k1.p, k2.p, v1.p, out.p, (int)n, 0, 6, st));
+    DBuf<uint8_t> tb(tmp, st);
+    TSR_CUDA(cub::DeviceRadixSort::SortPairs(tb.p, tmp, k1.p, k2.p, v1.p, out.p, (int)n, 0, 6, st));
+    return out;
+}
+
 }  // namespace
 
 // The field of all links (update == false), or an update of an existing
@@ -1105,6 +1134,7 @@ void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_
             TSR_CUDA(cub::DeviceSelect::Flagged(tb.p, tmp, ids.p, cflag.p, clist.p, nsel.p, (int)nl, st));
             const uint32_t nc = read_scalar(nsel.p, st);
             if (nc) {
+                clist = depth_ordered(nc, clist.p, t.leaf_node.p, t.depth.p, st);
                 DBuf<double2> bnd(nc, st);
                 next_link.zero();
                 k_priors_x<true><<<prior_grid, PT_BLOCK, 0, st>>>(nc, nn, clist.p, t.leaf_node.p, t.leaf_min.p,
@@ -1121,6 +1151,7 @@ void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_
             nq = read_scalar(nsel.p, st);
             o.pruned = nl - nq;
         }
+        list = depth_ordered(nq, list.p, t.leaf_node.p, t.depth.p, st);
         next_link.zero();
         k_priors_x<false><<<prior_grid, PT_BLOCK, 0, st>>>(nq, nn, list.p, t.leaf_node.p, t.leaf_min.p, t.depth.p,
                                                           t.nmin.p, recs.p, psum.p, t.root_size,
@@ -1157,8 +1188,9 @@ void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_
             const uint32_t nf = read_scalar(nsel.p, st);
             if (nf == 0) break;
             k_set_needed<<<grid_for(nf, BLK), BLK, 0, st>>>(nf, flist.p, need.p); ::tsr::note_launch();
+            DBuf<uint32_t> fq = depth_ordered(nf, flist.p, t.leaf_node.p, t.depth.p, st);
             next_link.zero();
-            k_priors_x<false><<<prior_grid, PT_BLOCK, 0, st>>>(nf, nn, flist.p, t.leaf_node.p, t.leaf_min.p,
+            k_priors_x<false><<<prior_grid, PT_BLOCK, 0, st>>>(nf, nn, fq.p, t.leaf_node.p, t.leaf_min.p,
                                                               t.depth.p, t.nmin.p, recs.p, psum.p, t.root_size,
                                                               p.relative_radius_for_priors, o.prior.p, next_link.p,
                                                               accepted.p + 4, err.p, nullptr, 0); ::tsr::note_launch();
