@@ -55,7 +55,7 @@ L2_BYTES = 126 * 1024 * 1024
 # the cone passes, per leaf for the priors -- from one ncu capture of each
 # kernel on the 1M-sample CSG workload; the per-unit traffic is flat in the
 # size (one read of the per-link records and of the prior table)
-TRAFFIC_PER_UNIT = {"occ.sampleness": 160.0, "occ.emptiness": 161.1, "occ.priors": 169.5}
+TRAFFIC_PER_UNIT = {"occ.sampleness": 160.0, "occ.emptiness": 161.1, "occ.priors": 158.3}
 CPU_SAMPLE_N = 60_000     # the oracle port's sample (fp64_check)
 REF_SAMPLE_N = 3_000      # the reference build's sample per timed step (~4-6 s on 8-16 host threads)
 
