@@ -1213,7 +1213,9 @@ void build_tree(tsr_tree &t, const tsr_samples_view &sv, bool on_device) {
                 k_sens<<<grid_for(m, 128), 128, 0, st>>>(m, keys.p, v, root, pos.p, nrm.p, scale.p, h_svo, status.p,
                                                         witness.p, dleaf.p, soff.p, skeys.p, svals.p, margin,
                                                         derr.p); ::tsr::note_launch();
-                sort_pairs(skeys.p, ssorted.p, svals.p, by_leaf.p, nsens, st);
+                int leaf_bits = 1;   // node indices stay below the node count
+                while (leaf_bits < 32 && (1ull << leaf_bits) < (uint64_t)S.count) ++leaf_bits;
+                sort_pairs(skeys.p, ssorted.p, svals.p, by_leaf.p, nsens, st, leaf_bits);
                 k_segments<<<grid_for(nsens, BLK), BLK, 0, st>>>(nsens, ssorted.p, seg_lo.p, seg_hi.p); ::tsr::note_launch();
             }
             // waves: the frontier starts with every writer
