@@ -14,7 +14,7 @@ target is stated at; its samples are rendered on the GPU before timing.
   (tsr_tree_build_device), CUDA events on the launching stream: the plain
   FP32 path.
 * ``pruned`` -- the same steps with the learned pruner's field
-  (tsr_occupancy_compute_pruned), judged by the plain method on this scene.
+  (tsr_occupancy_compute_pruned), compared with the plain field on this scene.
 * ``e2e``    -- the plain step through the C ABI from pinned host buffers:
   H2D of the samples and the cameras, the tree build, the reordered samples
   copied back (the reference reorders Samples in place), the field, DMC and
@@ -525,7 +525,7 @@ def our_arm(args):
             "accepted_pairs_per_s": {"sampleness": oc.accepted_sampleness / (stages["occ.sampleness"] / 1e3),
                                      "emptiness": oc.accepted_emptiness / (stages["occ.emptiness"] / 1e3)}},
     }
-    # ---- the learned pruner's field (same workload, same timing), judged by
+    # ---- the learned pruner's field (same workload, same timing), compared with
     # the plain method on this scene
     pr = None
     if not args.no_pruned:
@@ -550,7 +550,7 @@ def our_arm(args):
         jt = core.Tree(core.Samples(host["pos"].numpy(), host["nrm"].numpy(), host["scale"].numpy(),
                                     host["conf"].numpy(), host["links"].numpy().view(np.uint32)), params,
                        stream=stream, reorder_samples=False)
-        j = pruner_mod.judge(jt, cams, pr, params, stream=stream)
+        j = pruner_mod.compare_with_plain(jt, cams, pr, params, stream=stream)
         del jt
         line["pruned"] = {
             "value": world_samples * args.steps / t_pruned, "unit": UNIT, "ms_per_step": 1e3 * t_pruned / args.steps,
@@ -559,7 +559,7 @@ def our_arm(args):
             "skipped_prior_queries": poc.pruned_leaves, "repaired_leaves": poc.repaired_leaves,
             "certified_skips": poc.certified_leaves, "leaves": int(Nl),
             "stage_ms": {k: round(float(v), 3) for k, v in zip(names, pstage / args.steps) if k},
-            "judge": {"sign_agreement": j["sign_agreement"], "case_agreement": j["case_agreement"],
+            "vs_plain": {"sign_agreement": j["sign_agreement"], "case_agreement": j["case_agreement"],
                       "vertex_hausdorff": j["vertex_hausdorff"], "finest_leaf_size": j["finest_leaf_size"],
                       "triangles_plain_pruned": j["triangles"], "visited_plain_pruned": j["visited"]},
             "network": pr.describe(),

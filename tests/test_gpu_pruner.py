@@ -1,4 +1,4 @@
-"""The pruned field with the committed trained network, judged by the plain
+"""The pruned field with the committed trained network, compared with the plain
 method on a scene the network never saw (random CSG scene, seed 500).
 
 What the network gains over the method without it: the prior queries of
@@ -30,9 +30,9 @@ def test_pruned_field_matches_plain_mesh_with_less_work(heldout):
     from tsr_b200 import core, pruner
     tree, cams = heldout
     from fieldcheck import log
-    j = pruner.judge(tree, cams, core.Pruner.load())
+    j = pruner.compare_with_plain(tree, cams, core.Pruner.load())
     saved = 1.0 - j["visited"]["visited_priors"][1] / j["visited"]["visited_priors"][0]
-    log({"test": "pruner_judge", "prior_work_saved": saved, **j})
+    log({"test": "pruner_vs_plain", "prior_work_saved": saved, **j})
     assert j["case_agreement"] >= MIN_CASE_AGREEMENT, j
     assert j["vertex_hausdorff"] <= MAX_HAUSDORFF_LEAVES * j["finest_leaf_size"], j
     assert saved >= MIN_PRIOR_WORK_SAVED, j
@@ -64,8 +64,8 @@ def test_pruned_field_is_exact_on_a_cluttered_scene():
     from tsr_b200 import core, pruner, scenes
     sc = scenes.cluttered_scene(seed=4, n_target=150_000, width=384, height=216, f=280.0, n_cams=60)
     tree = core.Tree(core.Samples.from_scene(sc), reorder_samples=False)
-    j = pruner.judge(tree, core.Cameras(sc.cams), core.Pruner.load())
-    log({"test": "pruner_judge_cluttered", **j})
+    j = pruner.compare_with_plain(tree, core.Cameras(sc.cams), core.Pruner.load())
+    log({"test": "pruner_vs_plain_cluttered", **j})
     assert j["sign_agreement"] == 1.0, j
     assert j["case_agreement"] == 1.0, j
     assert j["vertex_hausdorff"] == 0.0, j
@@ -100,8 +100,8 @@ def test_network_against_certifying_every_leaf(heldout):
     alone = core.Pruner.load()
     alone.band_threshold = 0.999999
     alone.sign_threshold = 0.4999
-    jn = pruner.judge(tree, cams, net)
-    ja = pruner.judge(tree, cams, alone)
+    jn = pruner.compare_with_plain(tree, cams, net)
+    ja = pruner.compare_with_plain(tree, cams, alone)
     log({"test": "network_vs_certify_all", "network": jn["visited"]["visited_priors"],
          "certify_all": ja["visited"]["visited_priors"], "pruned": [jn["pruned_leaves"], ja["pruned_leaves"]]})
     for j in (jn, ja):

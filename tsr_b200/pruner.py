@@ -212,8 +212,8 @@ def emptiness_needed_fraction(tree, plain, pruned, rel_radius=25.0):
     return {"leaves": float(needed.mean()), "kernel_sum": float(e[got][needed].sum() / e[got].sum())}
 
 
-def judge(tree, cams, pruner, params=None, stream=None):
-    """The plain method judges the pruned field: both fields and meshes on
+def compare_with_plain(tree, cams, pruner, params=None, stream=None):
+    """The pruned field against the plain one: both fields and meshes on
     the same tree, with the pruned field's error and work savings."""
     plain = core.Occupancy(tree, cams, params, stream=stream)
     mesh_plain = plain.extractCrust()
