@@ -560,8 +560,8 @@ def our_arm(args):
             "certified_skips": poc.certified_leaves, "leaves": int(Nl),
             "stage_ms": {k: round(float(v), 3) for k, v in zip(names, pstage / args.steps) if k},
             "vs_plain": {"sign_agreement": j["sign_agreement"], "case_agreement": j["case_agreement"],
-                      "vertex_hausdorff": j["vertex_hausdorff"], "finest_leaf_size": j["finest_leaf_size"],
-                      "triangles_plain_pruned": j["triangles"], "visited_plain_pruned": j["visited"]},
+                         "vertex_hausdorff": j["vertex_hausdorff"], "finest_leaf_size": j["finest_leaf_size"],
+                         "triangles_plain_pruned": j["triangles"], "visited_plain_pruned": j["visited"]},
             "network": pr.describe(),
         }
     else:
