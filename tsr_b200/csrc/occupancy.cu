@@ -548,7 +548,11 @@ __global__ void __launch_bounds__(PT_BLOCK, (TYPE == 0) ? TSR_CONE_E_BLOCKS : TS
 }
 
 // Pruned field repair: skipped reliable leaves (need == 0, E + S >= the
-// threshold) that border a leaf of the other sign.
+// threshold) that are positive and share a face with a negative leaf.  DMC
+// interpolates along dual-cell edges, which join face neighbours, so only
+// the values at the two ends of a sign change matter, and the negative end's
+// value is -EPS whatever its prior (Occupancy.cpp:570-587): the positive end
+// alone needs its exact prior.
 __global__ void k_repair_mark(uint32_t nl, const uint32_t *nb_off, const uint32_t *nbs, const double *occ,
                               const uint8_t *need, const double *esum, const double *ssum, double threshold,
                               uint8_t *mark) {
@@ -559,8 +563,8 @@ __global__ void k_repair_mark(uint32_t nl, const uint32_t *nb_off, const uint32_
     for (uint32_t e = nb_off[l]; e < nb_off[l + 1]; ++e) {
         const uint32_t m = nbs[e];
         if ((occ[m] > 0.0) == pl) continue;
-        if (skipped(l)) mark[l] = 1;
-        if (skipped(m)) mark[m] = 1;
+        const uint32_t positive = pl ? l : m;
+        if (skipped(positive)) mark[positive] = 1;
     }
 }
 
@@ -1171,9 +1175,10 @@ void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_
                                                  p.confidence_threshold, pred, need.p, o.e_sum.p, o.s_sum.p,
                                                  o.e_len.p, o.s_len.p, o.occ.p); ::tsr::note_launch();
     if (pred) {
-        // Repair: a skipped leaf that borders a sign change after all was
-        // predicted wrongly, or its value matters to the surface; query its
-        // prior and recompute it, until no skipped leaf borders a sign change.
+        // Repair: a skipped positive leaf next to a negative one carries a
+        // value the surface uses (the signs themselves are exact); query its
+        // prior and recompute it, until no such leaf is left (one round
+        // queries them all; the next finds none).
         DBuf<uint8_t> mark(nl, st);
         DBuf<uint32_t> ids(nl, st), flist(nl, st), nsel(1, st);
         k_iota<<<grid_for(nl, BLK), BLK, 0, st>>>(nl, ids.p); ::tsr::note_launch();
