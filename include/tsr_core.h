@@ -114,7 +114,7 @@ typedef struct {
     uint64_t visited_emptiness;        /* ... EMPTINESS pass */
     uint64_t visited_priors;           /* tree nodes classified by the prior sphere queries */
     uint64_t pruned_leaves;            /* prior queries the pruned field skipped (0 for the plain field) */
-    uint64_t repaired_leaves;          /* skipped positive leaves queried after all: they share a face with a negative leaf */
+    uint64_t repaired_leaves;          /* skipped positive leaves queried after all: next to a negative leaf, side of EPSILON unproved */
     uint64_t certified_leaves;         /* skip candidates whose sign bounds of their prior proved */
 } tsr_occupancy_counts;
 
@@ -343,11 +343,13 @@ TSR_API tsr_status tsr_mlp_infer_bf16(const float *x, uint32_t n, const float *p
  * undecided), and is skipped only when
  * the bounds prove its sign ((1 - p) S > p E for every p in them, or for
  * none); it then takes that sign, with the value 0.5 (S - E) / coneCount
- * when positive, and its prior reads NaN.  A skipped positive leaf that
- * shares a face with a negative one is queried after all (a negative leaf's
- * value is -EPSILON with or without its prior).  So every sign is the plain
- * field's, and both ends of every sign change have the plain field's
- * values: the DMC mesh equals the plain field's. */
+ * when positive (moved to 2 EPSILON or to EPSILON when the bounds prove the
+ * exact value above EPSILON or at most EPSILON), and its prior reads NaN.
+ * A skipped positive leaf that shares a face with a negative one is queried
+ * after all unless that side of EPSILON is proved (a negative leaf's value
+ * is -EPSILON with or without its prior, and DMC snaps a vertex to an end
+ * within EPSILON of zero).  So every sign is the plain field's and every
+ * vertex the plain field's: the DMC mesh equals the plain field's. */
 TSR_API tsr_status tsr_occupancy_compute_pruned(const tsr_tree *tree, const tsr_cameras_view *cameras,
                                                 const tsr_params *params, const tsr_pruner *pruner,
                                                 void *cuda_stream, tsr_occupancy **out_occupancy);

@@ -24,6 +24,8 @@ constexpr uint32_t FLAG_EMPTINESS = 2u;            // Occupancy.h:39
 // per-leaf predictions of the learned pruner: near a sign change (or within
 // the dilation ring), confidently positive, confidently not positive
 constexpr uint8_t PRED_KEEP = 1, PRED_POS = 2, PRED_NEG = 4;
+// A certified positive leaf whose value is proved above EPSILON / at most EPSILON.
+constexpr uint8_t PRED_HIGH = 8, PRED_LOW = 16;
 constexpr int MAX_TREE_DEPTH = 40;                 // stack bound of the traversals
 
 struct Error {

@@ -225,8 +225,15 @@ __global__ void k_prior_needed(uint32_t nl, const uint8_t *pred, const double *e
 // margin of 1e-9 that covers the rounding of the sums and of the exact
 // formula; otherwise the leaf is queried (need 1).  A certified leaf's sign
 // goes to its PRED_POS / PRED_NEG bits, which the pruned k_finalize uses.
+//
+// A positive leaf's value (1 - p) S / coneCount - p E / coneCount is also
+// placed against EPSILON when the bounds decide it (PRED_HIGH / PRED_LOW,
+// same margin): DMC snaps a vertex to the end of an edge whose value is
+// within EPSILON of zero, and a negative leaf's value is -EPSILON, so that
+// side is all the mesh takes from a positive leaf's value.
 __global__ void k_certify(uint32_t n, const uint32_t *list, const double *esum, const double *ssum,
-                          const double2 *bounds, uint8_t *pred, uint8_t *need, unsigned long long *certified) {
+                          const double2 *bounds, const double *cone_count, uint8_t *pred, uint8_t *need,
+                          unsigned long long *certified) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     bool ok = false;
     if (i < n) {
@@ -234,10 +241,13 @@ __global__ void k_certify(uint32_t n, const uint32_t *list, const double *esum, 
         const double e = esum[l], s = ssum[l];
         const double2 b = bounds[i];
         const double margin = 1e-9 * (s + e);
-        const bool pos = (1.0 - b.y) * s - b.y * e > margin;
-        const bool neg = (1.0 - b.x) * s - b.x * e < -margin;
+        const double at_hi = (1.0 - b.y) * s - b.y * e, at_lo = (1.0 - b.x) * s - b.x * e;
+        const bool pos = at_hi > margin;
+        const bool neg = at_lo < -margin;
         const uint8_t keep = pred[l] & PRED_KEEP;
-        if (pos) pred[l] = keep | PRED_POS;
+        const double eps_cc = EPS * *cone_count;
+        if (pos) pred[l] = keep | PRED_POS | (at_hi > eps_cc + margin ? PRED_HIGH : 0) |
+                           (at_lo < eps_cc - margin ? PRED_LOW : 0);
         else if (neg) pred[l] = keep | PRED_NEG;
         ok = pos || neg;
         need[l] = ok ? NEED_NONE : NEED_QUERY;
@@ -548,17 +558,21 @@ __global__ void __launch_bounds__(PT_BLOCK, (TYPE == 0) ? TSR_CONE_E_BLOCKS : TS
 }
 
 // Pruned field repair: skipped reliable leaves (need == 0, E + S >= the
-// threshold) that are positive and share a face with a negative leaf.  DMC
-// interpolates along dual-cell edges, which join face neighbours, so only
-// the values at the two ends of a sign change matter, and the negative end's
-// value is -EPS whatever its prior (Occupancy.cpp:570-587): the positive end
-// alone needs its exact prior.
+// threshold) that are positive and share a face with a negative leaf, and
+// whose value's side of EPSILON is not proved.  DMC interpolates along
+// dual-cell edges, which join face neighbours, so only the two ends of a
+// sign change matter; the negative end's value is -EPS whatever its prior
+// (Occupancy.cpp:570-587), and with one end at -EPS the vertex snaps to an
+// end, decided by whether the positive end's value exceeds EPS
+// (DualMarchingCell.cpp:51-71).
 __global__ void k_repair_mark(uint32_t nl, const uint32_t *nb_off, const uint32_t *nbs, const double *occ,
-                              const uint8_t *need, const double *esum, const double *ssum, double threshold,
-                              uint8_t *mark) {
+                              const uint8_t *need, const uint8_t *pred, const double *esum, const double *ssum,
+                              double threshold, uint8_t *mark) {
     uint32_t l = blockIdx.x * blockDim.x + threadIdx.x;
     if (l >= nl) return;
-    auto skipped = [&](uint32_t x) { return !need[x] && !((esum[x] + ssum[x]) < threshold); };
+    auto skipped = [&](uint32_t x) {
+        return !need[x] && !((esum[x] + ssum[x]) < threshold) && !(pred[x] & (PRED_HIGH | PRED_LOW));
+    };
     const bool pl = occ[l] > 0.0;
     for (uint32_t e = nb_off[l]; e < nb_off[l + 1]; ++e) {
         const uint32_t m = nbs[e];
@@ -929,7 +943,12 @@ __global__ void k_finalize(uint32_t nl, const double *esum, const double *ssum, 
     } else if (pred && !need[l]) {
         const bool pos = (e == 0.0) ? true : (s == 0.0) ? false : (pred[l] & PRED_POS) != 0;
         const double approx = 0.5 * (s - e) / cone_count;
-        v = (pos && approx > 0.0) ? approx : (pos ? EPS : -EPS);
+        if (pos && (pred[l] & PRED_HIGH))
+            v = approx > 2.0 * EPS ? approx : 2.0 * EPS;   // above EPSILON, like the exact value
+        else if (pos && (pred[l] & PRED_LOW))
+            v = EPS;                                       // at most EPSILON, like the exact value
+        else
+            v = (pos && approx > 0.0) ? approx : (pos ? EPS : -EPS);
     } else {
         double pr = prior[l];
         double pe = pr * (e / cone_count);
@@ -1146,7 +1165,8 @@ void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_
                                                                   p.relative_radius_for_priors, nullptr, next_link.p,
                                                                   accepted.p + 4, err.p, bnd.p, pruner->bound_levels);
                 ::tsr::note_launch();
-                k_certify<<<grid_for(nc, BLK), BLK, 0, st>>>(nc, clist.p, esum, ssum, bnd.p, pred_buf.p, need.p,
+                k_certify<<<grid_for(nc, BLK), BLK, 0, st>>>(nc, clist.p, esum, ssum, bnd.p, cone_count.p,
+                                                            pred_buf.p, need.p,
                                                             ncert.p); ::tsr::note_launch();
                 o.certified = read_scalar(ncert.p, st);
             }
@@ -1187,7 +1207,7 @@ void compute_occupancy(const tsr_tree &t, const tsr_cameras_view &cv, const tsr_
         DBuf<uint8_t> tb(tmp, st);
         for (int round = 0; round < 64; ++round) {
             mark.zero();
-            k_repair_mark<<<grid_for(nl, BLK), BLK, 0, st>>>(nl, t.nb_off.p, t.nbs.p, o.occ.p, need.p, esum, ssum,
+            k_repair_mark<<<grid_for(nl, BLK), BLK, 0, st>>>(nl, t.nb_off.p, t.nbs.p, o.occ.p, need.p, pred, esum, ssum,
                                                             p.confidence_threshold, mark.p); ::tsr::note_launch();
             TSR_CUDA(cub::DeviceSelect::Flagged(tb.p, tmp, ids.p, mark.p, flist.p, nsel.p, (int)nl, st));
             const uint32_t nf = read_scalar(nsel.p, st);
